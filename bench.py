@@ -1,0 +1,526 @@
+#!/usr/bin/env python
+"""Benchmark of the GeRaF RF operators on B200.
+
+Headline (one JSON line on rank 0): matched-filter backprojection throughput in
+G (voxel x antenna x sample) per second on the full-size workload -- 49152
+virtual channels (64 x 64 scan x 3TX4RX), 256 ADC samples per chirp, a 128^3
+voxel volume over a cube-shell + torus scene of 30k point scatterers at 20 dB
+SNR (synthetic: the reference's RF data is not released) -- in the MIXED
+arithmetic form (FP64 phase reduction, FP32 Horner phasors, compensated sums).
+
+One step = one backprojection of the whole volume with inputs resident in HBM
+(``value``); ``e2e`` repeats it through the public ``matched_filter_cuda`` call
+from pinned host buffers with the host->device copies and the result read-back
+inside the timed region.  Under torchrun each rank backprojects its own 128^3
+slab of a taller volume (weak scaling, no collective on the data path).
+
+Also reported: the FP32-pipe roofline of the kernel (algorithmic 8 flops per
+voxel-antenna-sample over the measured FP32 FMA rate), the PLAIN form on a
+voxel subset, the MF adjoint, the tracer forward + adjoint in rays/s, relative
+L2 errors against the FP64 oracle, clocks during the timed region, and the CPU
+baseline (the reference-order FP32 oracle port on the host cores).
+
+``--impl reference`` times the reference's CPU path -- here the FP32
+reference-order restatement in oracle/ (the reference has no CPU code; its CUDA
+kernels are the GPU parity pin) -- on a bounded voxel sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "geraf-sens_b200")]
+
+METRIC = "MF backprojection Gvox·ant·samp/s; tracer fwd+bwd rays/s; rel err vs FP64"
+UNIT = "Gvox·ant·samp/s"
+FLOPS_PER_TRIPLE = 8  # one complex multiply-accumulate of an IF sample by a unit phasor
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["mf-full", "mf-small"], default="mf-full")
+    ap.add_argument("--precision", choices=["mixed", "plain"], default="mixed")
+    ap.add_argument("--no-extras", action="store_true", help="headline only (for profiling)")
+    ap.add_argument("--seed", type=int, default=0)
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock, power and throttle reasons every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "-i", str(gpu_index),
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = []
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), max=float(parts[2]),
+                                 power=float(parts[3]) if parts[3] not in ("[N/A]", "N/A") else 0.0,
+                                 hw=parts[5], hwt=parts[6], swt=parts[7], swp=parts[8]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        loaded = [r for r in rows if r["power"] > 250.0] or rows
+        sm = sorted(r["sm"] for r in loaded)
+        reasons = set()
+        for r in loaded:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                              ("swt", "sw_thermal_slowdown"), ("swp", "sw_power_cap")):
+                if r[key].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r["max"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows), "samples_under_load": len(loaded),
+                "power_w_max": max(r["power"] for r in rows)}
+
+
+# ---------------------------------------------------------------------------
+def fp32_peak_tflops(dev) -> float:
+    """Measured FP32 FMA rate of this GPU (the roofline denominator)."""
+    import torch
+
+    from geraf_b200 import _lib
+
+    lib = _lib.load()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    blocks, threads, iters = sms * 8, 256, 1 << 15
+    sink = torch.empty(blocks * threads, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    best = 0.0
+    for _ in range(4):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        _lib.check(lib.geraf_rf_fma_probe(blocks, threads, iters, sink.data_ptr(), stream), "probe")
+        e.record()
+        e.synchronize()
+        ms = s.elapsed_time(e)
+        best = max(best, blocks * threads * iters * 16 / (ms * 1e-3) / 1e12)
+    return best
+
+
+def make_mf_workload(name, rank, world, dev, seed):
+    import numpy as np
+    import torch
+
+    from geraf_b200 import scenes
+
+    w = scenes.mf_full_workload(seed) if name == "mf-full" else scenes.mf_small_workload(seed)
+    vox = w["voxel"].copy()
+    span = float(vox[2].max() - vox[2].min()) + (vox[2, 1] - vox[2, 0] if vox.shape[1] > 1 else 0.0)
+    vox[2] += rank * (span if span > 0 else 0.0)  # rank r backprojects slab r of a taller volume
+    tx = torch.tensor(w["tx"], device=dev)
+    rx = torch.tensor(w["rx"], device=dev)
+    gen = torch.Generator(device=dev).manual_seed(seed + 1)
+    re, im = scenes.synthesize_if(tx, rx, torch.tensor(w["positions"]), torch.tensor(w["amplitudes"]),
+                                  w["chirp"], snr_db=w["snr_db"], generator=gen)
+    return dict(tx=tx, rx=rx, real=re, imag=im, voxel=torch.tensor(vox, device=dev), chirp=w["chirp"],
+                A=tx.shape[0], S=w["chirp"].num_samples, N=vox.shape[1], positions=w["positions"])
+
+
+def mf_call(wl, out_r, out_i, precision, voxel=None, N=None):
+    from geraf_b200.ops.RFMatchedFilter import _C
+
+    ch = wl["chirp"]
+    vox = wl["voxel"] if voxel is None else voxel
+    n = wl["N"] if N is None else N
+    _C.MatchedFilter_forward(wl["real"], wl["imag"], wl["tx"], wl["rx"], out_r, out_i, vox, wl["A"],
+                             wl["S"], ch.adc_sample_rate, ch.As_sci, n, precision=precision)
+
+
+def launches_per_mf_call(wl, precision) -> int:
+    from geraf_b200 import _lib
+
+    mode = _lib.MODE_MIXED if precision == "mixed" else _lib.MODE_PLAIN
+    ws = _lib.workspace_bytes("geraf_mf_forward_workspace_bytes", wl["A"], wl["S"], wl["N"],
+                              _lib.DTYPE_F32, mode, None)
+    return 2 if ws > 0 else 1
+
+
+def read_profile_traffic(workload: str):
+    """DRAM bytes per launch of the MF forward from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"mf_forward_mixed_{workload.replace('-', '_')}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from geraf_b200 import _lib
+
+    _lib.load()
+    wl = make_mf_workload(args.workload, rank, world, dev, args.seed)
+    A, S, N = wl["A"], wl["S"], wl["N"]
+    triples = float(A) * S * N
+    out_r = torch.empty(N, device=dev)
+    out_i = torch.empty(N, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    # warm-up (also resolves launch shapes, module loading and the status word)
+    for _ in range(max(args.warmup, 1)):
+        mf_call(wl, out_r, out_i, args.precision)
+    torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(local)
+    kernel_ms = []
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        flush.fill_(1.0)  # L2 flush between steps (256 MiB write)
+        ks, ke = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ks.record(stream)
+        mf_call(wl, out_r, out_i, args.precision)
+        ke.record(stream)
+        kernel_ms.append((ks, ke))
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clock_info = clocks.stop()
+    total_ms = max_over_ranks(t0.elapsed_time(t1), world)
+    kms = float(np.mean([a.elapsed_time(b) for a, b in kernel_ms]))
+    value = world * triples / (total_ms * 1e-3 / args.steps) / 1e9
+
+    # end to end through the public API, host buffers in, host result out
+    from geraf_b200.ops.RFMatchedFilter import matched_filter_cuda
+
+    ch = wl["chirp"]
+    h_re = wl["real"].cpu().pin_memory()
+    h_im = wl["imag"].cpu().pin_memory()
+    h_tx = wl["tx"].cpu().pin_memory()
+    h_rx = wl["rx"].cpu().pin_memory()
+    h_vox = wl["voxel"].t().contiguous().cpu().pin_memory()  # the API takes [N, 3]
+    h_out_r = torch.empty(N, pin_memory=True)
+    h_out_i = torch.empty(N, pin_memory=True)
+    h2d = sum(t.numel() * t.element_size() for t in (h_re, h_im, h_tx, h_rx, h_vox))
+    d2h = 2 * N * 4
+
+    def e2e_step():
+        yr, yi = matched_filter_cuda(h_re.to(dev, non_blocking=True), h_im.to(dev, non_blocking=True),
+                                     h_tx.to(dev, non_blocking=True), h_rx.to(dev, non_blocking=True),
+                                     h_vox.to(dev, non_blocking=True), A, S, ch.adc_sample_rate,
+                                     ch.As_sci, N, precision=args.precision)
+        h_out_r.copy_(yr, non_blocking=True)
+        h_out_i.copy_(yi, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize(dev)
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world) / e2e_steps
+    e2e_value = world * triples / (e2e_ms * 1e-3) / 1e9
+
+    peak = fp32_peak_tflops(dev)
+    achieved = FLOPS_PER_TRIPLE * triples / (kms * 1e-3) / 1e12
+    traffic = read_profile_traffic(args.workload)
+    launches = launches_per_mf_call(wl, args.precision) * args.steps
+
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded point-scatterer scene; reference RF data not released)",
+        "config": {
+            "workload": (f"{args.workload}: {A} virtual channels x {S} ADC samples x {N} voxels "
+                         f"per GPU ({args.precision} form)"),
+            "antennas": A, "samples": S, "voxels_per_gpu": N, "precision": args.precision,
+            "phase_reduction": "f64" if args.precision == "mixed" else "f32 (reference order)",
+            "l2": "flushed between timed steps (256 MiB write)",
+            "parallelism": f"voxel slabs x{world}, no collective",
+        },
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
+        "roofline": {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 3),
+                     "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "flops_per_launch": FLOPS_PER_TRIPLE * triples,
+                     "peak_source": "measured FP32 FMA rate (geraf_rf_fma_probe) in this process",
+                     "kernel_ms": round(kms, 3)},
+        "gpu_launches": launches,
+        "clocks": clock_info,
+    }
+
+    if rank == 0 and not args.no_extras:
+        line.update(extras(args, wl, dev, out_r, out_i))
+        if world == 1:
+            line["cpu_baseline"], line["rel_err_vs_fp64"] = cpu_leg(wl, out_r, out_i, dev)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def extras(args, wl, dev, out_r, out_i) -> dict:
+    """Secondary measurements: PLAIN form, MF adjoint, tracer fwd+adjoint."""
+    import torch
+
+    from geraf_b200 import autotune
+    from geraf_b200.ops.RFMatchedFilter import _C as mfc
+    from geraf_b200.ops.RFSignalTracer import _C as trc
+    from geraf_b200.sdf import tracer_workload
+
+    res = {}
+    A, S, N = wl["A"], wl["S"], wl["N"]
+    ch = wl["chirp"]
+    # PLAIN form on a voxel subset (it evaluates sinf/cosf per triple)
+    n_sub = min(N, 16384)
+    vsub = wl["voxel"][:, :n_sub].contiguous()
+    pr = torch.empty(n_sub, device=dev)
+    pi = torch.empty(n_sub, device=dev)
+    mf_call(wl, pr, pi, "plain", voxel=vsub, N=n_sub)
+    ms = autotune.time_call(lambda: mf_call(wl, pr, pi, "plain", voxel=vsub, N=n_sub), iters=1, warmup=0)
+    res["plain_form"] = {"value": round(float(A) * S * n_sub / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                         "voxels": n_sub, "ms": round(ms, 2)}
+    # MF adjoint (mixed) on the full workload
+    g_r = torch.randn(N, device=dev)
+    g_i = torch.randn(N, device=dev)
+    h_r = torch.empty((A, S), device=dev)
+    h_i = torch.empty((A, S), device=dev)
+
+    def adj():
+        mfc.MatchedFilter_backward_realimag(g_r, g_i, wl["real"], wl["imag"], wl["tx"], wl["rx"], h_r,
+                                            h_i, wl["voxel"], A, S, ch.adc_sample_rate, ch.As_sci, N,
+                                            precision="mixed")
+
+    ms = autotune.time_call(adj, iters=1, warmup=1)
+    res["mf_adjoint"] = {"value": round(float(A) * S * N / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                         "ms": round(ms, 2), "precision": "mixed"}
+    # tracer forward + adjoint: 64 antennas x 4096 rays x 128 samples, S = 128
+    tw = tracer_workload(device=dev, seed=args.seed)
+    At, P, St = tw["A"], tw["P"], tw["chirp"].num_samples
+    cfg = tw["radar_cfg"]
+    xr = torch.empty((At, St), device=dev)
+    xi = torch.empty((At, St), device=dev)
+    gxr = torch.randn((At, St), device=dev)
+    gxi = torch.randn((At, St), device=dev)
+    gn = torch.empty((P, 3), device=dev)
+    gs = torch.empty((At, P), device=dev)
+    gp = torch.empty((P, 3), device=dev)
+    tr = {}
+    for prec in ("mixed", "plain"):
+        def step(prec=prec):
+            trc.SignalTracer_forward(tw["normals"], tw["sigmas"], tw["points"], tw["tx"], tw["rx"],
+                                     tw["inbounds"], xr, xi, St, cfg["adcSampleRate"], cfg["fc_start"],
+                                     cfg["As_sci"], At, P, precision=prec)
+            trc.SignalTracer_backward_normal_sigma(gxr, gxi, tw["normals"], tw["sigmas"], tw["points"],
+                                                   tw["tx"], tw["rx"], tw["inbounds"], gn, gs, St,
+                                                   cfg["adcSampleRate"], cfg["fc_start"], cfg["As_sci"],
+                                                   At, P, grad_points=gp if prec == "mixed" else None,
+                                                   precision=prec)
+        ms = autotune.time_call(step, iters=3 if prec == "mixed" else 1, warmup=1)
+        tr[prec] = {"rays_per_s": round(At * tw["rays"] / (ms * 1e-3), 1), "ms": round(ms, 3),
+                    "gpts_per_s": round(float(At) * P * St / (ms * 1e-3) / 1e9, 2)}
+    res["tracer"] = {"workload": f"{At} antennas x {tw['rays']} rays x {P // tw['rays']} samples, S={St}",
+                     "unit": "rays/s (ray = ray x antenna pair)", "mixed_with_point_grads": tr["mixed"],
+                     "plain": tr["plain"]}
+    return res
+
+
+def cpu_leg(wl, out_r, out_i, dev):
+    """CPU baseline (reference-order FP32 oracle port, all host threads) on a
+    bounded voxel sample, and FP64-oracle errors of both forms on sampled voxels."""
+    import numpy as np
+    import torch
+
+    from oracle import rf_oracle as orc
+
+    ch = wl["chirp"]
+    A, S, N = wl["A"], wl["S"], wl["N"]
+    re = wl["real"].cpu().numpy()
+    im = wl["imag"].cpu().numpy()
+    tx = wl["tx"].cpu().numpy()
+    rx = wl["rx"].cpu().numpy()
+    vox = wl["voxel"].cpu().numpy()
+    # calibrate a sample that takes ~10 s
+    rng = np.random.default_rng(7)
+    n0 = 8
+    idx = rng.choice(N, n0, replace=False)
+    t = time.perf_counter()
+    orc.mf_forward(re, im, tx, rx, vox[:, idx], ch.adc_sample_rate, ch.As_sci, "f32")
+    dt0 = time.perf_counter() - t
+    n = int(max(n0, min(4096, n0 * 10.0 / max(dt0, 1e-3))))
+    n = max(orc.num_threads(), (n // orc.num_threads()) * orc.num_threads())
+    idx = rng.choice(N, n, replace=False)
+    t = time.perf_counter()
+    orc.mf_forward(re, im, tx, rx, vox[:, idx], ch.adc_sample_rate, ch.As_sci, "f32")
+    dt = time.perf_counter() - t
+    cpu = {"value": round(float(A) * S * n / dt / 1e9, 4), "unit": UNIT, "cores": orc.num_threads(),
+           "kind": "port",
+           "sample": f"{n} random voxels x {A} antennas x {S} samples ({dt:.1f} s), FP32 reference order"}
+    # errors vs FP64 on the 16 brightest voxels + 48 random ones
+    mag = torch.hypot(out_r, out_i).cpu().numpy()
+    pick = np.unique(np.concatenate([np.argsort(mag)[-16:], rng.choice(N, 48, replace=False)]))
+    fr, fi = orc.mf_forward(re, im, tx, rx, vox[:, pick], ch.adc_sample_rate, ch.As_sci, "f64")
+    ref = fr + 1j * fi
+    ours = out_r.cpu().numpy()[pick] + 1j * out_i.cpu().numpy()[pick]
+    pr = torch.empty(len(pick), device=dev)
+    pi = torch.empty(len(pick), device=dev)
+    mf_call(wl, pr, pi, "plain", voxel=wl["voxel"][:, torch.tensor(pick, device=dev)].contiguous(), N=len(pick))
+    plain = pr.cpu().numpy() + 1j * pi.cpu().numpy()
+
+    def rel(a):
+        return float(np.linalg.norm(a - ref) / np.linalg.norm(ref))
+
+    errs = {"mf_forward_mixed": rel(ours), "mf_forward_plain": rel(plain),
+            "voxels": int(len(pick)), "how": "16 brightest + 48 random voxels vs the FP64 oracle"}
+    return cpu, errs
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    """Times the reference's arithmetic on the host cores (the FP32
+    reference-order oracle port; the reference ships no CPU implementation)."""
+    import numpy as np
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    from geraf_b200 import scenes
+    from oracle import rf_oracle as orc
+
+    w = scenes.mf_full_workload(args.seed) if args.workload == "mf-full" else scenes.mf_small_workload(args.seed)
+    ch = w["chirp"]
+    A, S = w["tx"].shape[0], ch.num_samples
+    N = w["voxel"].shape[1]
+    rng = np.random.default_rng(args.seed)
+    # the cost is independent of the sample values: seeded Gaussian IF of the workload's shape
+    re = rng.standard_normal((A, S)).astype(np.float32)
+    im = rng.standard_normal((A, S)).astype(np.float32)
+    idx = rng.choice(N, 8, replace=False)
+    t = time.perf_counter()
+    orc.mf_forward(re, im, w["tx"], w["rx"], w["voxel"][:, idx], ch.adc_sample_rate, ch.As_sci, "f32")
+    dt0 = time.perf_counter() - t
+    threads = orc.num_threads()
+    n = int(max(threads, min(2048, 8 * 8.0 / max(dt0, 1e-3))))
+    n = max(threads, (n // threads) * threads)
+    times = []
+    for step in range(args.warmup + args.steps):
+        idx = rng.choice(N, n, replace=False)
+        t = time.perf_counter()
+        orc.mf_forward(re, im, w["tx"], w["rx"], w["voxel"][:, idx], ch.adc_sample_rate, ch.As_sci, "f32")
+        if step >= args.warmup:
+            times.append(time.perf_counter() - t)
+    sec = float(np.mean(times))
+    value = float(A) * S * n / sec / 1e9
+    sample = (f"{n} random voxels of {N} x {A} antennas x {S} samples per step, "
+              f"FP32 reference-order port, {threads} threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.workload}: {A} virtual channels x {S} ADC samples x {N} voxels",
+                   "antennas": A, "samples": S, "voxels": N},
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

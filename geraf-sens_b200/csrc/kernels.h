@@ -1,0 +1,129 @@
+// Internal launch interface between the C ABI layer (capi.cu) and the kernel
+// translation units.  Sizes are validated by the caller before any launcher
+// runs; launchers only pick launch shapes, enqueue kernels and report the
+// launch status.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace geraf {
+
+enum DType : int { kF32 = 0, kF64 = 1, kF16 = 2 };
+enum Mode : int { kPlain = 0, kMixed = 1 };
+
+struct Tuning {
+  int threads = 0;
+  int items = 0;       // voxels / points per thread
+  int stage_rows = 0;  // antenna rows per shared-memory stage
+  int splits = 0;      // partial-sum splits of the reduced dimension
+  int chunk = 0;       // samples per lane (sample-major kernels)
+};
+
+struct DeviceInfo {
+  int sm_count;
+  int max_smem_optin;
+};
+DeviceInfo current_device_info();
+
+// Device address of the library's status word on the current device
+// (looked up once per device; null if the lookup failed).
+int* device_status_ptr();
+
+// ---- matched filter ------------------------------------------------------
+struct MfArgs {
+  const void* real;
+  const void* imag;
+  const void* tx;
+  const void* rx;
+  void* out_real;
+  void* out_imag;
+  const void* voxel;  // [3, N]
+  const void* grad_real_out;  // backward: [N]
+  const void* grad_imag_out;
+  int64_t A, S, N;
+  float fs, As;
+  int dtype, mode;
+};
+
+Tuning mf_forward_resolve(const MfArgs& a, const Tuning& req);
+size_t mf_forward_workspace(const MfArgs& a, const Tuning& t);
+cudaError_t mf_forward(const MfArgs& a, const Tuning& t, void* ws, cudaStream_t st);
+
+Tuning mf_backward_resolve(const MfArgs& a, const Tuning& req);
+size_t mf_backward_workspace(const MfArgs& a, const Tuning& t);
+cudaError_t mf_backward(const MfArgs& a, const Tuning& t, void* ws, cudaStream_t st);
+
+struct MfFftArgs {
+  const void* real;  // forward: [A, bins] spectrum; backward: unused
+  const void* imag;
+  const void* tx;
+  const void* rx;
+  void* out_real;  // forward: [N]; backward: [A, bins]
+  void* out_imag;
+  const void* voxel;
+  const void* grad_real_out;  // backward: [N]
+  const void* grad_imag_out;
+  int64_t A, bins, N;
+  float spacing;
+  int dtype;
+};
+cudaError_t mf_fft_forward(const MfFftArgs& a, cudaStream_t st);
+cudaError_t mf_fft_backward(const MfFftArgs& a, cudaStream_t st);
+
+// ---- signal tracer ------------------------------------------------------
+struct TracerArgs {
+  const void* normals;  // [P,3]
+  const void* sigmas;   // [A,P]
+  const void* points;   // [P,3]
+  const void* tx;       // [A,3]
+  const void* rx;
+  const uint8_t* inbounds;  // [P]
+  void* out_real;  // forward: [A,S]
+  void* out_imag;
+  const void* grad_real_out;  // backward: [A,S]
+  const void* grad_imag_out;
+  void* grad_normals;  // backward: [P,3]
+  void* grad_sigmas;   // backward: [A,P]
+  void* grad_points;   // backward: [P,3] or null
+  int64_t A, S, P;
+  float fs, f0, As;
+  int dtype, mode;
+};
+
+Tuning tracer_forward_resolve(const TracerArgs& a, const Tuning& req);
+size_t tracer_forward_workspace(const TracerArgs& a, const Tuning& t);
+cudaError_t tracer_forward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st);
+
+Tuning tracer_backward_resolve(const TracerArgs& a, const Tuning& req);
+size_t tracer_backward_workspace(const TracerArgs& a, const Tuning& t);
+cudaError_t tracer_backward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st);
+
+struct BilinearArgs {
+  const void* normals;  // fwd: [R,S,3] in; bwd: grad_output_normals [R,T,3]
+  const void* sigmas;   // fwd: [A,R,S] in; bwd: grad_output_sigmas [A,R,T]
+  const void* z_vals;   // [R,S]
+  const void* tz_vals;  // [R,T]
+  void* out_normals;    // fwd: [R,T,3]; bwd: grad_normals [R,S,3] (accumulated)
+  void* out_sigmas;     // fwd: [A,R,T]; bwd: grad_sigmas [A,R,S] (accumulated)
+  uint8_t* out_inbounds;  // fwd: [R,T]
+  int64_t A, R, S, T;
+  int dtype;
+};
+cudaError_t bilinear_forward(const BilinearArgs& a, cudaStream_t st);
+cudaError_t bilinear_backward(const BilinearArgs& a, cudaStream_t st);
+
+// ---- shared host helpers -------------------------------------------------
+// FP64 phase constants of the MIXED form for start frequency f0, chirp slope
+// As, sample rate fs (see path_cycles in common.cuh).
+struct PhaseConsts {
+  double k0, b0, k1, b1;
+};
+PhaseConsts phase_consts(float f0, float As, float fs);
+
+// Picks the number of splits of the reduced dimension so that
+// `units * splits` blocks fill the GPU in near-whole waves.
+int pick_splits(int64_t units, int blocks_per_sm, int sm_count, int64_t max_splits);
+
+}  // namespace geraf

@@ -1,0 +1,910 @@
+// Matched-filter backprojection (RFMatchedFilter) kernels for sm_100a.
+//
+// Forward  y[v]   = (1/A) sum_a sum_n s[a,n] exp(-j phi(a,v,n))       (voxel-major)
+// Adjoint  g[a,n] = (1/A) sum_v G[v]   exp(+j phi(a,v,n))             (sample-major)
+// with phi(a,v,n) = 2 pi f0 tau(a,v) + 2 pi As (n/fs) tau(a,v), f0 = 773.704,
+// tau = (|tx_a - v| + |rx_a - v| + 0.15) / 2.9979
+// (reference: geraf/ops/RFMatchedFilter/csrc/matched_filter/MatchedFilter_cuda_kernel.cu:28-115,171-220).
+//
+// PLAIN kernels evaluate the reference's FP32 expressions per (v, a, n) with
+// accurate cosf/sinf and keep the reference's per-output summation order, so
+// their outputs track the reference to the last few ulps; their speed comes
+// from TMA-staged sample tiles, a per-sample constant table and per-(v,a)
+// geometry hoisting.
+//
+// MIXED kernels use that phi is linear in n: with z = exp(-j 2 pi dcyc) the
+// forward inner sum is exp(-j phi0) * P_a(z), P_a(z) = sum_n s[a,n] z^n,
+// evaluated by Horner (4 FMA per sample); the adjoint generates
+// G[v] exp(j phi0) zeta^n by a rotator recurrence.  phi0 is reduced modulo one
+// cycle in FP64 (path_cycles), so only two phasors per (v, a) are evaluated.
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace geraf {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Shared-memory layout of the voxel-major forward kernels.
+struct FwdSmem {
+  size_t pos_off, kn_off, buf_off, total;
+};
+
+template <typename T, typename PosT>
+FwdSmem fwd_smem_layout(int rows, int ld, bool with_kn) {
+  FwdSmem s;
+  s.pos_off = 128;  // two mbarriers, padded
+  size_t off = s.pos_off + 2 * static_cast<size_t>(rows) * 6 * sizeof(PosT);
+  off = (off + 127) & ~static_cast<size_t>(127);
+  s.kn_off = off;
+  if (with_kn) off += static_cast<size_t>(ld) * sizeof(float);
+  off = (off + 127) & ~static_cast<size_t>(127);
+  s.buf_off = off;
+  off += 4 * static_cast<size_t>(rows) * ld * sizeof(T);
+  s.total = (off + 127) & ~static_cast<size_t>(127);
+  return s;
+}
+
+template <typename T>
+struct MfFwdP {
+  const T* real;
+  const T* imag;
+  const T* tx;
+  const T* rx;
+  T* out_r;
+  T* out_i;
+  const T* voxel;
+  float2* partial;  // [splits][N] when splits > 1
+  int* status;
+  int64_t A, S, N;
+  float fs, As;
+  double k0, b0, k1, b1;
+  int rows, ld, splits, bulk;
+  int64_t ant_per_split;
+  size_t pos_off, kn_off, buf_off;
+};
+
+__device__ __forceinline__ float sq(float x) { return x * x; }
+
+// Stages antenna positions of one tile as PosT (float for PLAIN, double for MIXED).
+template <typename T, typename PosT>
+__device__ __forceinline__ void stage_positions(PosT* pos, int stage, int rows_max, const T* tx,
+                                                const T* rx, int64_t a0, int rws) {
+  for (int i = threadIdx.x; i < rws * 6; i += blockDim.x) {
+    const int r = i / 6;
+    const int c = i - r * 6;
+    const T* src = c < 3 ? tx : rx;
+    pos[(stage * rows_max + r) * 6 + c] = static_cast<PosT>(ld_f(src, (a0 + r) * 3 + (c % 3)));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MIXED forward: VPT voxels per thread, antennas streamed through a
+// double-buffered TMA ring of `rows` antennas x S samples.
+template <typename T, int VPT>
+__global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  double* pos = reinterpret_cast<double*>(smem + p.pos_off);
+  PairStager<T> stg{reinterpret_cast<T*>(smem + p.buf_off), bar, p.ld, p.rows, p.bulk != 0};
+
+  const int split = blockIdx.x % p.splits;
+  const int64_t vtile = blockIdx.x / p.splits;
+  const int64_t a_begin = static_cast<int64_t>(split) * p.ant_per_split;
+  const int64_t a_end = min(p.A, a_begin + p.ant_per_split);
+  const int ntiles = a_end > a_begin ? ceil_div(a_end - a_begin, p.rows) : 0;
+
+  if (p.bulk && threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  double vx[VPT], vy[VPT], vz[VPT];
+  int64_t vid[VPT];
+#pragma unroll
+  for (int j = 0; j < VPT; ++j) {
+    vid[j] = vtile * blockDim.x * VPT + threadIdx.x + static_cast<int64_t>(j) * blockDim.x;
+    const bool ok = vid[j] < p.N;
+    vx[j] = ok ? static_cast<double>(ld_f(p.voxel, vid[j])) : 0.0;
+    vy[j] = ok ? static_cast<double>(ld_f(p.voxel, p.N + vid[j])) : 0.0;
+    vz[j] = ok ? static_cast<double>(ld_f(p.voxel, 2 * p.N + vid[j])) : 0.0;
+  }
+  float yr[VPT], yi[VPT], cr[VPT], ci[VPT];
+#pragma unroll
+  for (int j = 0; j < VPT; ++j) yr[j] = yi[j] = cr[j] = ci[j] = 0.0f;
+
+  auto issue = [&](int tile, int stage) {
+    const int64_t a0 = a_begin + static_cast<int64_t>(tile) * p.rows;
+    const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
+    stg.issue(stage, p.real, p.imag, a0, rws, static_cast<int>(p.S));
+    stage_positions<T, double>(pos, stage, p.rows, p.tx, p.rx, a0, rws);
+  };
+  if (ntiles > 0) issue(0, 0);
+  if (ntiles > 1) issue(1, 1);
+
+  for (int t = 0; t < ntiles; ++t) {
+    const int s = t & 1;
+    if (!stg.wait(s, (t >> 1) & 1, p.status)) {
+      if (t + 1 < ntiles) stg.drain(s ^ 1, ((t + 1) >> 1) & 1, p.status);
+      return;
+    }
+    const int64_t a0 = a_begin + static_cast<int64_t>(t) * p.rows;
+    const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
+    const T* sre = stg.stage_ptr(s, 0);
+    const T* sim = stg.stage_ptr(s, 1);
+    for (int r = 0; r < rws; ++r) {
+      const double* ps = pos + (s * p.rows + r) * 6;
+      const double tx = ps[0], ty = ps[1], tz = ps[2], rx = ps[3], ry = ps[4], rz = ps[5];
+      float2 e0[VPT], z[VPT];
+      float pr[VPT], pi[VPT];
+#pragma unroll
+      for (int j = 0; j < VPT; ++j) {
+        const PhaseCycles pc = path_cycles(tx - vx[j], ty - vy[j], tz - vz[j], rx - vx[j],
+                                           ry - vy[j], rz - vz[j], p.k0, p.b0, p.k1, p.b1);
+        const float2 c0 = cis_cycles(pc.frac0);
+        const float2 c1 = cis_cycles(pc.dcyc);
+        e0[j] = make_float2(c0.x, -c0.y);  // exp(-j phi0)
+        z[j] = make_float2(c1.x, -c1.y);   // exp(-j dphi)
+        pr[j] = 0.0f;
+        pi[j] = 0.0f;
+      }
+      const T* rowr = sre + r * p.ld;
+      const T* rowi = sim + r * p.ld;
+      // Horner from the highest sample down: P <- P z + s[n].  Padded
+      // samples (n >= S) are zero and leave P at zero.
+#pragma unroll 2
+      for (int n = p.ld - 4; n >= 0; n -= 4) {
+        const float4 a = lds4(rowr + n);
+        const float4 b = lds4(rowi + n);
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) {
+          float nr, ni;
+          nr = fmaf(pr[j], z[j].x, fmaf(-pi[j], z[j].y, a.w));
+          ni = fmaf(pr[j], z[j].y, fmaf(pi[j], z[j].x, b.w));
+          pr[j] = nr; pi[j] = ni;
+          nr = fmaf(pr[j], z[j].x, fmaf(-pi[j], z[j].y, a.z));
+          ni = fmaf(pr[j], z[j].y, fmaf(pi[j], z[j].x, b.z));
+          pr[j] = nr; pi[j] = ni;
+          nr = fmaf(pr[j], z[j].x, fmaf(-pi[j], z[j].y, a.y));
+          ni = fmaf(pr[j], z[j].y, fmaf(pi[j], z[j].x, b.y));
+          pr[j] = nr; pi[j] = ni;
+          nr = fmaf(pr[j], z[j].x, fmaf(-pi[j], z[j].y, a.x));
+          ni = fmaf(pr[j], z[j].y, fmaf(pi[j], z[j].x, b.x));
+          pr[j] = nr; pi[j] = ni;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < VPT; ++j) {
+        const float2 term = cmul(e0[j], make_float2(pr[j], pi[j]));
+        kahan_add(yr[j], cr[j], term.x);
+        kahan_add(yi[j], ci[j], term.y);
+      }
+    }
+    __syncthreads();
+    if (t + 2 < ntiles) issue(t + 2, s);
+  }
+
+#pragma unroll
+  for (int j = 0; j < VPT; ++j) {
+    if (vid[j] >= p.N) continue;
+    if (p.splits == 1) {
+      p.out_r[vid[j]] = from_f<T>(yr[j] / static_cast<float>(p.A));
+      p.out_i[vid[j]] = from_f<T>(yi[j] / static_cast<float>(p.A));
+    } else {
+      p.partial[split * p.N + vid[j]] = make_float2(yr[j], yi[j]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PLAIN forward: the reference's per-(v, a, n) FP32 arithmetic
+// (MatchedFilter_cuda_kernel.cu:28-58, 86-114), one accumulator per voxel in
+// the reference's (a, n) order.
+template <typename T, int VPT>
+__global__ void __launch_bounds__(256) mf_fwd_plain_kernel(const MfFwdP<T> p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  float* pos = reinterpret_cast<float*>(smem + p.pos_off);
+  float* kn = reinterpret_cast<float*>(smem + p.kn_off);
+  PairStager<T> stg{reinterpret_cast<T*>(smem + p.buf_off), bar, p.ld, p.rows, p.bulk != 0};
+
+  const int split = blockIdx.x % p.splits;
+  const int64_t vtile = blockIdx.x / p.splits;
+  const int64_t a_begin = static_cast<int64_t>(split) * p.ant_per_split;
+  const int64_t a_end = min(p.A, a_begin + p.ant_per_split);
+  const int ntiles = a_end > a_begin ? ceil_div(a_end - a_begin, p.rows) : 0;
+  const int S = static_cast<int>(p.S);
+
+  if (p.bulk && threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_barrier_init();
+  }
+  // Per-sample factor of the reference's phase, 2*kPi*As*(n/fs), evaluated in
+  // the reference's order ((2*pi)*As)*t_n with t_n = float(n)/fs.
+  for (int n = threadIdx.x; n < p.ld; n += blockDim.x) {
+    const float sample_time = static_cast<float>(n) / p.fs;
+    kn[n] = 2.0f * kPiF * p.As * sample_time;
+  }
+  __syncthreads();
+
+  float vx[VPT], vy[VPT], vz[VPT];
+  int64_t vid[VPT];
+  float ar[VPT], ai[VPT];
+#pragma unroll
+  for (int j = 0; j < VPT; ++j) {
+    vid[j] = vtile * blockDim.x * VPT + threadIdx.x + static_cast<int64_t>(j) * blockDim.x;
+    const bool ok = vid[j] < p.N;
+    vx[j] = ok ? ld_f(p.voxel, vid[j]) : 0.0f;
+    vy[j] = ok ? ld_f(p.voxel, p.N + vid[j]) : 0.0f;
+    vz[j] = ok ? ld_f(p.voxel, 2 * p.N + vid[j]) : 0.0f;
+    ar[j] = 0.0f;
+    ai[j] = 0.0f;
+  }
+
+  auto issue = [&](int tile, int stage) {
+    const int64_t a0 = a_begin + static_cast<int64_t>(tile) * p.rows;
+    const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
+    stg.issue(stage, p.real, p.imag, a0, rws, S);
+    stage_positions<T, float>(pos, stage, p.rows, p.tx, p.rx, a0, rws);
+  };
+  if (ntiles > 0) issue(0, 0);
+  if (ntiles > 1) issue(1, 1);
+
+  for (int t = 0; t < ntiles; ++t) {
+    const int s = t & 1;
+    if (!stg.wait(s, (t >> 1) & 1, p.status)) {
+      if (t + 1 < ntiles) stg.drain(s ^ 1, ((t + 1) >> 1) & 1, p.status);
+      return;
+    }
+    const int64_t a0 = a_begin + static_cast<int64_t>(t) * p.rows;
+    const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
+    const T* sre = stg.stage_ptr(s, 0);
+    const T* sim = stg.stage_ptr(s, 1);
+    for (int r = 0; r < rws; ++r) {
+      const float* ps = pos + (s * p.rows + r) * 6;
+      const float tx_x = ps[0], tx_y = ps[1], tx_z = ps[2];
+      const float rx_x = ps[3], rx_y = ps[4], rx_z = ps[5];
+      const T* rowr = sre + r * p.ld;
+      const T* rowi = sim + r * p.ld;
+#pragma unroll
+      for (int j = 0; j < VPT; ++j) {
+        const float tx_distance = sqrtf(sq(tx_x - vx[j]) + sq(tx_y - vy[j]) + sq(tx_z - vz[j]));
+        const float rx_distance = sqrtf(sq(rx_x - vx[j]) + sq(rx_y - vy[j]) + sq(rx_z - vz[j]));
+        const float distance = tx_distance + rx_distance + kPathBias;
+        const float tau = distance / kSpeedOfLight;
+        const float base_phase = 2.0f * kPiF * kMfStartFrequency * tau;
+        float acc_r = ar[j], acc_i = ai[j];
+        for (int n = 0; n < S; ++n) {
+          const float phase = base_phase + kn[n] * tau;
+          const float cos_phase = cosf(phase);
+          const float neg_sin_phase = -sinf(phase);
+          const float sample_real = static_cast<float>(rowr[n]);
+          const float sample_imag = static_cast<float>(rowi[n]);
+          acc_r += cos_phase * sample_real - neg_sin_phase * sample_imag;
+          acc_i += cos_phase * sample_imag + neg_sin_phase * sample_real;
+        }
+        ar[j] = acc_r;
+        ai[j] = acc_i;
+      }
+    }
+    __syncthreads();
+    if (t + 2 < ntiles) issue(t + 2, s);
+  }
+
+  const int total_ant_size = static_cast<int>(p.A);
+#pragma unroll
+  for (int j = 0; j < VPT; ++j) {
+    if (vid[j] >= p.N) continue;
+    if (p.splits == 1) {
+      p.out_r[vid[j]] = from_f<T>(ar[j] / total_ant_size);
+      p.out_i[vid[j]] = from_f<T>(ai[j] / total_ant_size);
+    } else {
+      p.partial[split * p.N + vid[j]] = make_float2(ar[j], ai[j]);
+    }
+  }
+}
+
+// Sums `splits` partial rows of `count` complex values in a fixed order (FP64)
+// and divides by `divisor`.
+template <typename T>
+__global__ void finalize_partials_kernel(const float2* __restrict__ partial, int splits,
+                                         int64_t count, float divisor, T* out_r, T* out_i) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double sr = 0.0, si = 0.0;
+    for (int s = 0; s < splits; ++s) {
+      const float2 v = partial[s * count + i];
+      sr += v.x;
+      si += v.y;
+    }
+    out_r[i] = from_f<T>(static_cast<float>(sr) / divisor);
+    out_i[i] = from_f<T>(static_cast<float>(si) / divisor);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint kernels.
+template <typename T>
+struct MfBwdP {
+  const T* gr;  // [N]
+  const T* gi;
+  const T* tx;
+  const T* rx;
+  const T* voxel;
+  T* out_r;  // [A,S]
+  T* out_i;
+  float2* partial;  // [splits][A][S]
+  int64_t A, S, N;
+  float fs, As;
+  double k0, b0, k1, b1;
+  int splits;
+  int64_t vox_per_split;
+  int groups;  // sample groups per block
+};
+
+// MIXED adjoint.  Block = (antenna, voxel split, sample range).  Phase 1:
+// thread t forms w = G[v] exp(j phi0) and the group seeds w zeta^(g K) of
+// voxel v0 + t.  Phase 2: thread (group g, lane l) rotates seeds of its
+// lane's voxels through K samples, accumulating in registers; a two-level
+// FP32 sum (flushed per tile) bounds the error growth over long voxel ranges.
+template <typename T, int K>
+__global__ void __launch_bounds__(256) mf_bwd_mixed_kernel(const MfBwdP<T> p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int TILE = blockDim.x;
+  const int G = p.groups;
+  const int L = blockDim.x / G;
+  float2* seeds = reinterpret_cast<float2*>(smem);  // [G][TILE]
+  float2* zeta = seeds + static_cast<size_t>(G) * TILE;  // [TILE]
+
+  const int64_t a = blockIdx.x / p.splits;
+  const int split = blockIdx.x % p.splits;
+  const int64_t n_begin = static_cast<int64_t>(blockIdx.y) * G * K;
+  const int64_t v_begin = static_cast<int64_t>(split) * p.vox_per_split;
+  const int64_t v_end = min(p.N, v_begin + p.vox_per_split);
+
+  const double tx = ld_f(p.tx, a * 3 + 0), ty = ld_f(p.tx, a * 3 + 1), tz = ld_f(p.tx, a * 3 + 2);
+  const double rx = ld_f(p.rx, a * 3 + 0), ry = ld_f(p.rx, a * 3 + 1), rz = ld_f(p.rx, a * 3 + 2);
+
+  const int g = threadIdx.x / L;
+  const int l = threadIdx.x - g * L;
+  float accr[K], acci[K], hir[K], hii[K];
+#pragma unroll
+  for (int m = 0; m < K; ++m) accr[m] = acci[m] = hir[m] = hii[m] = 0.0f;
+
+  for (int64_t v0 = v_begin; v0 < v_end; v0 += TILE) {
+    {  // phase 1
+      const int64_t v = v0 + threadIdx.x;
+      float2 w = make_float2(0.0f, 0.0f), zt = make_float2(1.0f, 0.0f), zk = make_float2(1.0f, 0.0f);
+      if (v < v_end) {
+        const double vx = ld_f(p.voxel, v), vy = ld_f(p.voxel, p.N + v), vz = ld_f(p.voxel, 2 * p.N + v);
+        const PhaseCycles pc =
+            path_cycles(tx - vx, ty - vy, tz - vz, rx - vx, ry - vy, rz - vz, p.k0, p.b0, p.k1, p.b1);
+        float start = pc.frac0;
+        if (n_begin != 0) {
+          const double c = static_cast<double>(pc.frac0) + static_cast<double>(n_begin) * pc.dcyc;
+          start = static_cast<float>(c - rint(c));
+        }
+        const float2 e = cis_cycles(start);
+        const float2 gv = make_float2(ld_f(p.gr, v), ld_f(p.gi, v));
+        w = cmul(gv, e);
+        zt = cis_cycles(pc.dcyc);
+        const float kc = pc.dcyc * static_cast<float>(K);
+        zk = cis_cycles(kc - rintf(kc));
+      }
+      zeta[threadIdx.x] = zt;
+      for (int gg = 0; gg < G; ++gg) {
+        seeds[gg * TILE + threadIdx.x] = w;
+        w = cmul(w, zk);
+      }
+    }
+    __syncthreads();
+    {  // phase 2
+      const int count = static_cast<int>(min(static_cast<int64_t>(TILE), v_end - v0));
+      for (int vl = l; vl < count; vl += L) {
+        float2 s = seeds[g * TILE + vl];
+        const float2 z = zeta[vl];
+#pragma unroll
+        for (int m = 0; m < K; ++m) {
+          accr[m] += s.x;
+          acci[m] += s.y;
+          s = cmul(s, z);
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < K; ++m) {
+        hir[m] += accr[m];
+        hii[m] += acci[m];
+        accr[m] = acci[m] = 0.0f;
+      }
+    }
+    __syncthreads();
+  }
+
+  // Reduce the L lanes of each group through shared memory (fixed order).
+  float2* red = reinterpret_cast<float2*>(smem);  // [G][K][L]
+#pragma unroll
+  for (int m = 0; m < K; ++m) red[(g * K + m) * L + l] = make_float2(hir[m], hii[m]);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < G * K; idx += blockDim.x) {
+    const int64_t n = n_begin + idx;
+    if (n >= p.S) continue;
+    float sr = 0.0f, si = 0.0f;
+    for (int ll = 0; ll < L; ++ll) {
+      const float2 v = red[idx * L + ll];
+      sr += v.x;
+      si += v.y;
+    }
+    if (p.splits == 1) {
+      p.out_r[a * p.S + n] = from_f<T>(sr / static_cast<float>(p.A));
+      p.out_i[a * p.S + n] = from_f<T>(si / static_cast<float>(p.A));
+    } else {
+      p.partial[(split * p.A + a) * p.S + n] = make_float2(sr, si);
+    }
+  }
+}
+
+// PLAIN adjoint: thread = (antenna, sample), voxels in the reference's order
+// (MatchedFilter_cuda_kernel.cu:186-219).  Per-(a, v) path delays are formed
+// once per voxel tile in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(128) mf_bwd_plain_kernel(const MfBwdP<T> p) {
+  constexpr int TILE = 256;
+  __shared__ float s_tau[TILE], s_gr[TILE], s_gi[TILE];
+  const int64_t a = blockIdx.x;
+  const int64_t n = static_cast<int64_t>(blockIdx.y) * blockDim.x + threadIdx.x;
+  const bool active = n < p.S;
+  const float tx_x = ld_f(p.tx, a * 3 + 0), tx_y = ld_f(p.tx, a * 3 + 1), tx_z = ld_f(p.tx, a * 3 + 2);
+  const float rx_x = ld_f(p.rx, a * 3 + 0), rx_y = ld_f(p.rx, a * 3 + 1), rx_z = ld_f(p.rx, a * 3 + 2);
+  const float sample_time = static_cast<float>(n) / p.fs;
+  const float kn = 2.0f * kPiF * p.As * sample_time;
+  float acc_r = 0.0f, acc_i = 0.0f;
+  for (int64_t v0 = 0; v0 < p.N; v0 += TILE) {
+    const int count = static_cast<int>(min(static_cast<int64_t>(TILE), p.N - v0));
+    for (int i = threadIdx.x; i < count; i += blockDim.x) {
+      const int64_t v = v0 + i;
+      const float vx = ld_f(p.voxel, v), vy = ld_f(p.voxel, p.N + v), vz = ld_f(p.voxel, 2 * p.N + v);
+      const float tx_distance = sqrtf(sq(tx_x - vx) + sq(tx_y - vy) + sq(tx_z - vz));
+      const float rx_distance = sqrtf(sq(rx_x - vx) + sq(rx_y - vy) + sq(rx_z - vz));
+      const float distance = tx_distance + rx_distance + kPathBias;
+      s_tau[i] = distance / kSpeedOfLight;
+      s_gr[i] = ld_f(p.gr, v);
+      s_gi[i] = ld_f(p.gi, v);
+    }
+    __syncthreads();
+    if (active) {
+      for (int i = 0; i < count; ++i) {
+        const float tau = s_tau[i];
+        const float phase = 2.0f * kPiF * kMfStartFrequency * tau + kn * tau;
+        const float cos_phase = cosf(phase);
+        const float neg_sin_phase = -sinf(phase);
+        const float grad_real_out = s_gr[i];
+        const float grad_imag_out = s_gi[i];
+        acc_r += cos_phase * grad_real_out + neg_sin_phase * grad_imag_out;
+        acc_i += (-neg_sin_phase) * grad_real_out + cos_phase * grad_imag_out;
+      }
+    }
+    __syncthreads();
+  }
+  if (active) {
+    const int total_ant_size = static_cast<int>(p.A);
+    p.out_r[a * p.S + n] = from_f<T>(acc_r / total_ant_size);
+    p.out_i[a * p.S + n] = from_f<T>(acc_i / total_ant_size);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Range-bin (FFT) variants, reference arithmetic (MatchedFilter_cuda_kernel.cu:117-169, 222-279).
+template <typename T>
+struct MfFftP {
+  const T* real;
+  const T* imag;
+  const T* tx;
+  const T* rx;
+  const T* voxel;
+  const T* gr;
+  const T* gi;
+  T* out_r;
+  T* out_i;
+  int64_t A, bins, N;
+  float spacing;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) mf_fft_fwd_kernel(const MfFftP<T> p) {
+  const int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (v >= p.N) return;
+  const float vx = ld_f(p.voxel, v), vy = ld_f(p.voxel, p.N + v), vz = ld_f(p.voxel, 2 * p.N + v);
+  const int num_range_bins = static_cast<int>(p.bins);
+  float acc_r = 0.0f, acc_i = 0.0f;
+  for (int64_t a = 0; a < p.A; ++a) {
+    const float tx_x = ld_f(p.tx, a * 3 + 0), tx_y = ld_f(p.tx, a * 3 + 1), tx_z = ld_f(p.tx, a * 3 + 2);
+    const float rx_x = ld_f(p.rx, a * 3 + 0), rx_y = ld_f(p.rx, a * 3 + 1), rx_z = ld_f(p.rx, a * 3 + 2);
+    const float tx_distance = sqrtf(sq(tx_x - vx) + sq(tx_y - vy) + sq(tx_z - vz));
+    const float rx_distance = sqrtf(sq(rx_x - vx) + sq(rx_y - vy) + sq(rx_z - vz));
+    const float distance = tx_distance + rx_distance + kPathBias;
+    if (distance < 0.0f || distance > p.spacing * num_range_bins) continue;
+    const int range_bin = static_cast<int>(floorf(distance / p.spacing / 2.0f));
+    if (range_bin < 0 || range_bin >= num_range_bins) continue;
+    const float tau = distance / kSpeedOfLight;
+    const float phase = 2.0f * kPiF * kMfStartFrequency * tau;
+    const float cos_phase = cosf(phase);
+    const float neg_sin_phase = -sinf(phase);
+    const float sample_real = ld_f(p.real, a * p.bins + range_bin);
+    const float sample_imag = ld_f(p.imag, a * p.bins + range_bin);
+    acc_r += cos_phase * sample_real - neg_sin_phase * sample_imag;
+    acc_i += cos_phase * sample_imag + neg_sin_phase * sample_real;
+  }
+  const int total_ant_size = static_cast<int>(p.A);
+  p.out_r[v] = from_f<T>(acc_r / total_ant_size);
+  p.out_i[v] = from_f<T>(acc_i / total_ant_size);
+}
+
+// Adjoint: thread = (antenna, bin); per voxel tile the bin and delay of every
+// voxel are formed once in shared memory, then each thread gathers the voxels
+// of its bin in voxel order (the reference's order).
+template <typename T>
+__global__ void __launch_bounds__(128) mf_fft_bwd_kernel(const MfFftP<T> p) {
+  constexpr int TILE = 256;
+  __shared__ int s_bin[TILE];
+  __shared__ float s_tau[TILE], s_gr[TILE], s_gi[TILE];
+  const int64_t a = blockIdx.x;
+  const int64_t b = static_cast<int64_t>(blockIdx.y) * blockDim.x + threadIdx.x;
+  const int num_range_bins = static_cast<int>(p.bins);
+  const float tx_x = ld_f(p.tx, a * 3 + 0), tx_y = ld_f(p.tx, a * 3 + 1), tx_z = ld_f(p.tx, a * 3 + 2);
+  const float rx_x = ld_f(p.rx, a * 3 + 0), rx_y = ld_f(p.rx, a * 3 + 1), rx_z = ld_f(p.rx, a * 3 + 2);
+  float acc_r = 0.0f, acc_i = 0.0f;
+  for (int64_t v0 = 0; v0 < p.N; v0 += TILE) {
+    const int count = static_cast<int>(min(static_cast<int64_t>(TILE), p.N - v0));
+    for (int i = threadIdx.x; i < count; i += blockDim.x) {
+      const int64_t v = v0 + i;
+      const float vx = ld_f(p.voxel, v), vy = ld_f(p.voxel, p.N + v), vz = ld_f(p.voxel, 2 * p.N + v);
+      const float tx_distance = sqrtf(sq(tx_x - vx) + sq(tx_y - vy) + sq(tx_z - vz));
+      const float rx_distance = sqrtf(sq(rx_x - vx) + sq(rx_y - vy) + sq(rx_z - vz));
+      const float distance = tx_distance + rx_distance + kPathBias;
+      int bin = -1;
+      if (!(distance < 0.0f || distance > p.spacing * num_range_bins)) {
+        bin = static_cast<int>(floorf(distance / p.spacing / 2.0f));
+      }
+      s_bin[i] = bin;
+      s_tau[i] = distance / kSpeedOfLight;
+      s_gr[i] = ld_f(p.gr, v);
+      s_gi[i] = ld_f(p.gi, v);
+    }
+    __syncthreads();
+    if (b < p.bins) {
+      for (int i = 0; i < count; ++i) {
+        if (s_bin[i] != b) continue;
+        const float tau = s_tau[i];
+        const float phase = 2.0f * kPiF * kMfStartFrequency * tau;
+        const float cos_phase = cosf(phase);
+        const float neg_sin_phase = -sinf(phase);
+        const float grad_real_out = s_gr[i];
+        const float grad_imag_out = s_gi[i];
+        acc_r += cos_phase * grad_real_out + neg_sin_phase * grad_imag_out;
+        acc_i += (-neg_sin_phase) * grad_real_out + cos_phase * grad_imag_out;
+      }
+    }
+    __syncthreads();
+  }
+  if (b < p.bins) {
+    const int total_ant_size = static_cast<int>(p.A);
+    p.out_r[a * p.bins + b] = from_f<T>(acc_r / total_ant_size);
+    p.out_i[a * p.bins + b] = from_f<T>(acc_i / total_ant_size);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launch logic.
+size_t elem_size(int dtype) { return dtype == kF64 ? 8 : dtype == kF16 ? 2 : 4; }
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Forward shape: threads, voxels per thread, antenna rows per stage, splits.
+struct FwdShape {
+  int threads, vpt, rows, ld, splits;
+  int64_t ant_per_split;
+  bool bulk;
+  size_t smem;
+  FwdSmem layout;
+};
+
+template <typename T>
+const void* fwd_kernel_ptr(int mode, int vpt) {
+  if (mode == kMixed) {
+    if (vpt == 1) return reinterpret_cast<const void*>(&mf_fwd_mixed_kernel<T, 1>);
+    if (vpt == 2) return reinterpret_cast<const void*>(&mf_fwd_mixed_kernel<T, 2>);
+    return reinterpret_cast<const void*>(&mf_fwd_mixed_kernel<T, 4>);
+  }
+  if (vpt == 1) return reinterpret_cast<const void*>(&mf_fwd_plain_kernel<T, 1>);
+  if (vpt == 2) return reinterpret_cast<const void*>(&mf_fwd_plain_kernel<T, 2>);
+  return reinterpret_cast<const void*>(&mf_fwd_plain_kernel<T, 4>);
+}
+
+FwdShape fwd_shape(const MfArgs& a, const Tuning& t) {
+  FwdShape s;
+  s.threads = t.threads;
+  s.vpt = t.items;
+  s.splits = t.splits;
+  const size_t es = elem_size(a.dtype);
+  // TMA writes rows back to back, so the shared row stride must equal S.
+  s.bulk = (a.S > 0) && (a.S % 4 == 0) && ((a.S * es) % 16 == 0) && aligned16(a.real) &&
+           aligned16(a.imag);
+  s.ld = static_cast<int>(((std::max<int64_t>(a.S, 1) + 3) / 4) * 4);
+  s.rows = t.stage_rows;
+  const bool mixed = a.mode == kMixed;
+  auto layout = [&](int rows) {
+    if (a.dtype == kF64) return mixed ? fwd_smem_layout<double, double>(rows, s.ld, false)
+                                      : fwd_smem_layout<double, float>(rows, s.ld, true);
+    if (a.dtype == kF16) return mixed ? fwd_smem_layout<__half, double>(rows, s.ld, false)
+                                      : fwd_smem_layout<__half, float>(rows, s.ld, true);
+    return mixed ? fwd_smem_layout<float, double>(rows, s.ld, false)
+                 : fwd_smem_layout<float, float>(rows, s.ld, true);
+  };
+  const DeviceInfo dev = current_device_info();
+  s.layout = layout(s.rows);
+  while (s.rows > 1 && s.layout.total > static_cast<size_t>(dev.max_smem_optin)) {
+    s.rows /= 2;
+    s.layout = layout(s.rows);
+  }
+  s.smem = s.layout.total;
+  const int64_t rows_total = (a.A + s.rows - 1) / s.rows;
+  const int64_t rows_per_split = (rows_total + s.splits - 1) / s.splits;
+  s.ant_per_split = std::max<int64_t>(1, rows_per_split) * s.rows;
+  return s;
+}
+
+template <typename T>
+cudaError_t launch_fwd(const MfArgs& a, const FwdShape& s, void* ws, cudaStream_t st) {
+  MfFwdP<T> p;
+  p.real = static_cast<const T*>(a.real);
+  p.imag = static_cast<const T*>(a.imag);
+  p.tx = static_cast<const T*>(a.tx);
+  p.rx = static_cast<const T*>(a.rx);
+  p.out_r = static_cast<T*>(a.out_real);
+  p.out_i = static_cast<T*>(a.out_imag);
+  p.voxel = static_cast<const T*>(a.voxel);
+  p.partial = static_cast<float2*>(ws);
+  p.status = device_status_ptr();
+  p.A = a.A;
+  p.S = a.S;
+  p.N = a.N;
+  p.fs = a.fs;
+  p.As = a.As;
+  const PhaseConsts pc = phase_consts(kMfStartFrequency, a.As, a.fs);
+  p.k0 = pc.k0;
+  p.b0 = pc.b0;
+  p.k1 = pc.k1;
+  p.b1 = pc.b1;
+  p.rows = s.rows;
+  p.ld = s.ld;
+  p.splits = s.splits;
+  p.bulk = s.bulk ? 1 : 0;
+  p.ant_per_split = s.ant_per_split;
+  p.pos_off = s.layout.pos_off;
+  p.kn_off = s.layout.kn_off;
+  p.buf_off = s.layout.buf_off;
+
+  const void* fn = fwd_kernel_ptr<T>(a.mode, s.vpt);
+  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(s.smem));
+  if (err != cudaSuccess) return err;
+  const int64_t vtiles = (a.N + static_cast<int64_t>(s.threads) * s.vpt - 1) /
+                         (static_cast<int64_t>(s.threads) * s.vpt);
+  const int64_t blocks = vtiles * s.splits;
+  if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+  void* args[] = {&p};
+  err = cudaLaunchKernel(fn, dim3(static_cast<unsigned>(blocks)), dim3(s.threads), args, s.smem, st);
+  if (err != cudaSuccess) return err;
+  if (s.splits > 1) {
+    const int fin_blocks = static_cast<int>(std::min<int64_t>((a.N + 255) / 256, 148 * 16));
+    finalize_partials_kernel<T><<<std::max(fin_blocks, 1), 256, 0, st>>>(
+        p.partial, s.splits, a.N, static_cast<float>(a.A), p.out_r, p.out_i);
+    err = cudaGetLastError();
+  }
+  return err;
+}
+
+// Sample groups per block (a power of two, at most 64 so the seed table fits
+// in shared memory); longer sample axes are split over grid.y ranges.
+int bwd_groups(int64_t S, int chunk, int threads) {
+  const int64_t g = (S + chunk - 1) / chunk;
+  int groups = 1;
+  while (groups < g && groups < threads && groups < 64) groups *= 2;
+  return groups;
+}
+
+template <typename T, int K>
+cudaError_t launch_bwd_mixed_k(const MfBwdP<T>& p, dim3 grid, int threads, size_t smem,
+                               cudaStream_t st) {
+  const void* fn = reinterpret_cast<const void*>(&mf_bwd_mixed_kernel<T, K>);
+  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
+  void* args[] = {const_cast<MfBwdP<T>*>(&p)};
+  return cudaLaunchKernel(fn, grid, dim3(threads), args, smem, st);
+}
+
+size_t bwd_mixed_smem(int threads, int groups, int chunk) {
+  const size_t seeds = (static_cast<size_t>(groups) + 1) * threads * sizeof(float2);
+  const size_t red = static_cast<size_t>(threads) * chunk * sizeof(float2);
+  return std::max(seeds, red);
+}
+
+template <typename T>
+cudaError_t launch_bwd(const MfArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  MfBwdP<T> p;
+  p.gr = static_cast<const T*>(a.grad_real_out);
+  p.gi = static_cast<const T*>(a.grad_imag_out);
+  p.tx = static_cast<const T*>(a.tx);
+  p.rx = static_cast<const T*>(a.rx);
+  p.voxel = static_cast<const T*>(a.voxel);
+  p.out_r = static_cast<T*>(a.out_real);
+  p.out_i = static_cast<T*>(a.out_imag);
+  p.partial = static_cast<float2*>(ws);
+  p.A = a.A;
+  p.S = a.S;
+  p.N = a.N;
+  p.fs = a.fs;
+  p.As = a.As;
+  const PhaseConsts pc = phase_consts(kMfStartFrequency, a.As, a.fs);
+  p.k0 = pc.k0;
+  p.b0 = pc.b0;
+  p.k1 = pc.k1;
+  p.b1 = pc.b1;
+  p.splits = 1;
+  p.vox_per_split = a.N;
+  p.groups = 1;
+  if (a.mode == kPlain) {
+    const int threads = 128;
+    dim3 grid(static_cast<unsigned>(a.A), static_cast<unsigned>((a.S + threads - 1) / threads));
+    mf_bwd_plain_kernel<T><<<grid, threads, 0, st>>>(p);
+    return cudaGetLastError();
+  }
+  const int threads = t.threads;
+  const int chunk = t.chunk;
+  const int groups = bwd_groups(a.S, chunk, threads);
+  p.groups = groups;
+  p.splits = t.splits;
+  p.vox_per_split = (a.N + t.splits - 1) / t.splits;
+  const int64_t ranges = (a.S + static_cast<int64_t>(groups) * chunk - 1) /
+                         (static_cast<int64_t>(groups) * chunk);
+  dim3 grid(static_cast<unsigned>(a.A * t.splits), static_cast<unsigned>(ranges));
+  const size_t smem = bwd_mixed_smem(threads, groups, chunk);
+  cudaError_t err;
+  if (chunk == 8) err = launch_bwd_mixed_k<T, 8>(p, grid, threads, smem, st);
+  else if (chunk == 32) err = launch_bwd_mixed_k<T, 32>(p, grid, threads, smem, st);
+  else err = launch_bwd_mixed_k<T, 16>(p, grid, threads, smem, st);
+  if (err != cudaSuccess) return err;
+  if (t.splits > 1) {
+    const int64_t count = a.A * a.S;
+    const int fin_blocks = static_cast<int>(std::min<int64_t>((count + 255) / 256, 148 * 16));
+    finalize_partials_kernel<T><<<std::max(fin_blocks, 1), 256, 0, st>>>(
+        p.partial, t.splits, count, static_cast<float>(a.A), p.out_r, p.out_i);
+    err = cudaGetLastError();
+  }
+  return err;
+}
+
+template <typename T>
+cudaError_t launch_fft(const MfFftArgs& a, bool backward, cudaStream_t st) {
+  MfFftP<T> p;
+  p.real = static_cast<const T*>(a.real);
+  p.imag = static_cast<const T*>(a.imag);
+  p.tx = static_cast<const T*>(a.tx);
+  p.rx = static_cast<const T*>(a.rx);
+  p.voxel = static_cast<const T*>(a.voxel);
+  p.gr = static_cast<const T*>(a.grad_real_out);
+  p.gi = static_cast<const T*>(a.grad_imag_out);
+  p.out_r = static_cast<T*>(a.out_real);
+  p.out_i = static_cast<T*>(a.out_imag);
+  p.A = a.A;
+  p.bins = a.bins;
+  p.N = a.N;
+  p.spacing = a.spacing;
+  if (!backward) {
+    const int64_t blocks = (a.N + 255) / 256;
+    mf_fft_fwd_kernel<T><<<static_cast<unsigned>(blocks), 256, 0, st>>>(p);
+  } else {
+    dim3 grid(static_cast<unsigned>(a.A), static_cast<unsigned>((a.bins + 127) / 128));
+    mf_fft_bwd_kernel<T><<<grid, 128, 0, st>>>(p);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+Tuning mf_forward_resolve(const MfArgs& a, const Tuning& req) {
+  Tuning t = req;
+  if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 128;
+  if (t.items != 1 && t.items != 2 && t.items != 4) t.items = a.mode == kMixed ? 2 : 1;
+  if (t.stage_rows <= 0) t.stage_rows = 8;
+  t.stage_rows = std::min(t.stage_rows, 64);
+  const int64_t rows_total = std::max<int64_t>(1, (a.A + t.stage_rows - 1) / t.stage_rows);
+  if (t.splits <= 0) {
+    const int64_t vtiles = (a.N + static_cast<int64_t>(t.threads) * t.items - 1) /
+                           (static_cast<int64_t>(t.threads) * t.items);
+    const DeviceInfo dev = current_device_info();
+    const int per_sm = std::max(1, 1024 / t.threads);
+    t.splits = a.mode == kPlain ? 1 : pick_splits(vtiles, per_sm, dev.sm_count, rows_total);
+  }
+  t.splits = static_cast<int>(std::min<int64_t>(std::max(t.splits, 1), rows_total));
+  if (t.chunk <= 0) t.chunk = 16;
+  return t;
+}
+
+size_t mf_forward_workspace(const MfArgs& a, const Tuning& t) {
+  if (t.splits <= 1 || a.N == 0) return 0;
+  return static_cast<size_t>(t.splits) * a.N * sizeof(float2);
+}
+
+cudaError_t mf_forward(const MfArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  if (a.N == 0) return cudaSuccess;
+  const FwdShape s = fwd_shape(a, t);
+  switch (a.dtype) {
+    case kF64: return launch_fwd<double>(a, s, ws, st);
+    case kF16: return launch_fwd<__half>(a, s, ws, st);
+    default: return launch_fwd<float>(a, s, ws, st);
+  }
+}
+
+Tuning mf_backward_resolve(const MfArgs& a, const Tuning& req) {
+  Tuning t = req;
+  if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 256;
+  if (t.chunk != 8 && t.chunk != 16 && t.chunk != 32) t.chunk = 16;
+  if (t.items <= 0) t.items = 1;
+  if (t.stage_rows <= 0) t.stage_rows = 8;
+  if (a.mode == kPlain) {
+    t.splits = 1;
+    return t;
+  }
+  const int groups = bwd_groups(a.S, t.chunk, t.threads);
+  const int64_t ranges = (a.S + static_cast<int64_t>(groups) * t.chunk - 1) /
+                         (static_cast<int64_t>(groups) * t.chunk);
+  const int64_t vtiles = std::max<int64_t>(1, (a.N + t.threads - 1) / t.threads);
+  if (t.splits <= 0) {
+    const DeviceInfo dev = current_device_info();
+    const int per_sm = std::max(1, 512 / t.threads);
+    t.splits = pick_splits(std::max<int64_t>(1, a.A * ranges), per_sm, dev.sm_count, vtiles);
+  }
+  t.splits = static_cast<int>(std::min<int64_t>(std::max(t.splits, 1), vtiles));
+  return t;
+}
+
+size_t mf_backward_workspace(const MfArgs& a, const Tuning& t) {
+  if (a.mode == kPlain || t.splits <= 1) return 0;
+  return static_cast<size_t>(t.splits) * a.A * a.S * sizeof(float2);
+}
+
+cudaError_t mf_backward(const MfArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  if (a.A == 0 || a.S == 0) return cudaSuccess;
+  switch (a.dtype) {
+    case kF64: return launch_bwd<double>(a, t, ws, st);
+    case kF16: return launch_bwd<__half>(a, t, ws, st);
+    default: return launch_bwd<float>(a, t, ws, st);
+  }
+}
+
+cudaError_t mf_fft_forward(const MfFftArgs& a, cudaStream_t st) {
+  if (a.N == 0) return cudaSuccess;
+  switch (a.dtype) {
+    case kF64: return launch_fft<double>(a, false, st);
+    case kF16: return launch_fft<__half>(a, false, st);
+    default: return launch_fft<float>(a, false, st);
+  }
+}
+
+cudaError_t mf_fft_backward(const MfFftArgs& a, cudaStream_t st) {
+  if (a.A == 0 || a.bins == 0) return cudaSuccess;
+  switch (a.dtype) {
+    case kF64: return launch_fft<double>(a, true, st);
+    case kF16: return launch_fft<__half>(a, true, st);
+    default: return launch_fft<float>(a, true, st);
+  }
+}
+
+}  // namespace geraf

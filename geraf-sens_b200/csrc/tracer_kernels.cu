@@ -1,0 +1,1112 @@
+// Lensless specular signal tracer (RFSignalTracer) and along-ray resampler
+// kernels for sm_100a.
+//
+// Forward  x[a,n] = (1/P) sum_p amp(a,p) exp(+j (w0 + w1 t_n) tau(a,p))          (sample-major)
+// Adjoint  dL/dsigma[a,p], dL/dnormal[p], dL/dpoint[p]                             (point-major)
+// amp = sigma[a,p] rho / D^2, rho = <normalize(rx-p), normalize(i - 2(i.n)n)>,
+// i = normalize(p - tx), culled when rho < 1e-6 or i.n > 0, D = |tx-p| + |rx-p|,
+// tau = (D + 0.15)/2.9979, w0 = 2 pi f0, w1 = 2 pi As
+// (reference: geraf/ops/RFSignalTracer/csrc/signal_tracer/SignalTracer_cuda_kernel.cu:19-197, 351-587).
+//
+// The reference recomputes the specular geometry for every (point, antenna,
+// sample) triple.  Here the geometry is formed once per (point, antenna) --
+// in the reference's FP32 operation order, so amplitudes and culling decisions
+// are bit-identical -- and the sample loop works on (amplitude, delay) only.
+// PLAIN forms then evaluate the reference's per-sample phase with accurate
+// cosf/sinf in its summation order; MIXED forms reduce the carrier phase in
+// FP64 and generate the per-sample phasors with a rotator (forward) or a
+// Horner recurrence (adjoint), which also yields the position gradient the
+// reference does not provide.
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace geraf {
+namespace {
+
+__device__ __forceinline__ float sq(float x) { return x * x; }
+
+__device__ __forceinline__ float dot3(const float* a, const float* b) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+// normalize with the reference's epsilon: v / (|v| + 1e-7)
+__device__ __forceinline__ void normalize3(const float* in, float* out) {
+  const float norm = sqrtf(dot3(in, in));
+  const float inv_norm = 1.0f / (norm + kNormEps);
+  out[0] = in[0] * inv_norm;
+  out[1] = in[1] * inv_norm;
+  out[2] = in[2] * inv_norm;
+}
+
+// Specular geometry of one (point, antenna) pair in the reference's FP32
+// operation order (SignalTracer_cuda_kernel.cu:172-197).
+struct SpecGeom {
+  float inc[3];       // normalize(p - tx)
+  float refl_raw[3];  // inc - 2 (inc.n) n
+  float refl[3];      // normalize(refl_raw)
+  float ret[3];       // normalize(rx - p)
+  float align;        // rho
+  float idn;          // inc . n
+};
+
+__device__ __forceinline__ void specular_geometry(const float* tx, const float* rx, const float* nrm,
+                                                  const float* pt, SpecGeom& g) {
+  float inc_raw[3], ret_raw[3];
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    inc_raw[axis] = pt[axis] - tx[axis];
+    ret_raw[axis] = rx[axis] - pt[axis];
+  }
+  normalize3(inc_raw, g.inc);
+  g.idn = dot3(g.inc, nrm);
+  const float incident_dot_normal = dot3(g.inc, nrm);
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    g.refl_raw[axis] = g.inc[axis] - 2.0f * incident_dot_normal * nrm[axis];
+  }
+  normalize3(g.refl_raw, g.refl);
+  normalize3(ret_raw, g.ret);
+  g.align = dot3(g.ret, g.refl);
+}
+
+__device__ __forceinline__ bool culled(const SpecGeom& g) {
+  return g.align < 1.0e-6f || g.idn > 0.0f;
+}
+
+// |tx - p| + |rx - p| in the reference's order (ComputePathDistance).
+__device__ __forceinline__ float path_distance(const float* tx, const float* rx, const float* pt) {
+  return sqrtf(sq(tx[0] - pt[0]) + sq(tx[1] - pt[1]) + sq(tx[2] - pt[2])) +
+         sqrtf(sq(rx[0] - pt[0]) + sq(rx[1] - pt[1]) + sq(rx[2] - pt[2]));
+}
+
+// d rho / d n through the reflection and its normalisation, in the reference's
+// order (SignalTracer_cuda_kernel.cu:91-170, 531-542).
+__device__ __forceinline__ void align_normal_gradient(const SpecGeom& g, const float* nrm,
+                                                      float* gsa) {
+  const float incident_dot_normal = dot3(g.inc, nrm);
+  float jac[9];
+#pragma unroll
+  for (int row = 0; row < 3; ++row) {
+#pragma unroll
+    for (int col = 0; col < 3; ++col) {
+      const float shared_term = -2.0f * nrm[row] * g.inc[col];
+      jac[row * 3 + col] = row == col ? shared_term - 2.0f * incident_dot_normal : shared_term;
+    }
+  }
+  const float value_norm = sqrtf(dot3(g.refl_raw, g.refl_raw));
+  const float x = g.refl[0], y = g.refl[1], z = g.refl[2];
+  const float inv_norm = 1.0f / (value_norm + kNormEps);
+  float nj[9];
+  nj[0] = ((1.0f - x * x) * jac[0] + (-x * y) * jac[3] + (-x * z) * jac[6]) * inv_norm;
+  nj[1] = ((1.0f - x * x) * jac[1] + (-x * y) * jac[4] + (-x * z) * jac[7]) * inv_norm;
+  nj[2] = ((1.0f - x * x) * jac[2] + (-x * y) * jac[5] + (-x * z) * jac[8]) * inv_norm;
+  nj[3] = ((-y * x) * jac[0] + (1.0f - y * y) * jac[3] + (-y * z) * jac[6]) * inv_norm;
+  nj[4] = ((-y * x) * jac[1] + (1.0f - y * y) * jac[4] + (-y * z) * jac[7]) * inv_norm;
+  nj[5] = ((-y * x) * jac[2] + (1.0f - y * y) * jac[5] + (-y * z) * jac[8]) * inv_norm;
+  nj[6] = ((-z * x) * jac[0] + (-z * y) * jac[3] + (1.0f - z * z) * jac[6]) * inv_norm;
+  nj[7] = ((-z * x) * jac[1] + (-z * y) * jac[4] + (1.0f - z * z) * jac[7]) * inv_norm;
+  nj[8] = ((-z * x) * jac[2] + (-z * y) * jac[5] + (1.0f - z * z) * jac[8]) * inv_norm;
+#pragma unroll
+  for (int axis = 0; axis < 3; ++axis) {
+    float value = 0.0f;
+#pragma unroll
+    for (int component = 0; component < 3; ++component) {
+      value += nj[component * 3 + axis] * g.ret[component];
+    }
+    gsa[axis] = value;
+  }
+}
+
+// d rho / d p (no reference counterpart): rho = <o, r/|r|>, r = H i, H = I - 2 n n^T,
+// i = (p - tx)/|p - tx|, o = (rx - p)/|rx - p|.
+__device__ __forceinline__ void align_point_gradient(const SpecGeom& g, const float* nrm, float dist_t,
+                                                     float dist_r, float* out) {
+  const float rnorm = sqrtf(dot3(g.refl_raw, g.refl_raw));
+  const float ro = dot3(g.refl, g.ret);
+  float u[3], v[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) u[k] = (g.ret[k] - g.refl[k] * ro) / rnorm;
+  const float nu = dot3(nrm, u);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) v[k] = u[k] - 2.0f * nu * nrm[k];
+  const float iv = dot3(g.inc, v);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float w = (v[k] - g.inc[k] * iv) / dist_t;
+    const float q = -(g.refl[k] - g.ret[k] * ro) / dist_r;
+    out[k] = w + q;
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <typename T>
+struct TrP {
+  const T* normals;
+  const T* sigmas;
+  const T* points;
+  const T* tx;
+  const T* rx;
+  const uint8_t* inb;
+  T* out_r;
+  T* out_i;
+  const T* gr;
+  const T* gi;
+  T* g_normals;
+  T* g_sigmas;
+  T* g_points;
+  float* partial;  // forward: [splits][A][S][2]; adjoint: [splits][P][6]
+  int* status;
+  int64_t A, S, P;
+  float fs, f0, As;
+  float phase_base, phase_slope;  // 2*kPi*f0 and 2*kPi*As in FP32, as the reference forms them
+  double k0, b0, k1, b1;
+  int splits;
+  int64_t per_split;  // points (forward) or antennas (adjoint) per split
+  int groups;         // forward: sample groups per block
+  int rows, ld, bulk;  // adjoint: antenna stage
+  size_t pos_off, buf_off;
+};
+
+template <typename T>
+__device__ __forceinline__ void load3(const T* base, int64_t i, float* out) {
+  out[0] = ld_f(base, i * 3 + 0);
+  out[1] = ld_f(base, i * 3 + 1);
+  out[2] = ld_f(base, i * 3 + 2);
+}
+
+// PLAIN forward: block = (sample block, antenna).  Per point tile, the
+// (amplitude, delay) of each point is formed once in shared memory; each
+// thread then accumulates its sample over the tile in point order, with the
+// reference's phase expression and accurate cosf/sinf
+// (SignalTracer_cuda_kernel.cu:375-449).
+template <typename T>
+__global__ void __launch_bounds__(128) tracer_fwd_plain_kernel(const TrP<T> p) {
+  constexpr int TILE = 256;
+  __shared__ float s_amp[TILE], s_tau[TILE];
+  __shared__ int s_valid[TILE];
+  const int64_t a = blockIdx.x;
+  const int64_t n = static_cast<int64_t>(blockIdx.y) * blockDim.x + threadIdx.x;
+  const bool active = n < p.S;
+  float txp[3], rxp[3];
+  load3(p.tx, a, txp);
+  load3(p.rx, a, rxp);
+  const float sample_time = static_cast<float>(n) / p.fs;
+  const float phase_base = p.phase_base;
+  const float phase_slope = p.phase_slope;
+  float acc_r = 0.0f, acc_i = 0.0f;
+  for (int64_t p0 = 0; p0 < p.P; p0 += TILE) {
+    const int count = static_cast<int>(min(static_cast<int64_t>(TILE), p.P - p0));
+    for (int i = threadIdx.x; i < count; i += blockDim.x) {
+      const int64_t pi = p0 + i;
+      int valid = 0;
+      float amp = 0.0f, tau = 0.0f;
+      if (p.inb[pi]) {
+        float nrm[3], pt[3];
+        load3(p.normals, pi, nrm);
+        load3(p.points, pi, pt);
+        SpecGeom g;
+        specular_geometry(txp, rxp, nrm, pt, g);
+        if (!culled(g)) {
+          float propagation_distance = path_distance(txp, rxp, pt);
+          amp = ld_f(p.sigmas, a * p.P + pi) * g.align / sq(propagation_distance);
+          propagation_distance += kPathBias;
+          tau = propagation_distance / kSpeedOfLight;
+          valid = 1;
+        }
+      }
+      s_valid[i] = valid;
+      s_amp[i] = amp;
+      s_tau[i] = tau;
+    }
+    __syncthreads();
+    if (active) {
+      for (int i = 0; i < count; ++i) {
+        if (!s_valid[i]) continue;
+        const float phase = (phase_base + phase_slope * sample_time) * s_tau[i];
+        acc_r += s_amp[i] * cosf(phase);
+        acc_i += s_amp[i] * sinf(phase);
+      }
+    }
+    __syncthreads();
+  }
+  if (active) {
+    const int total_point_size = static_cast<int>(p.P);
+    p.out_r[a * p.S + n] = from_f<T>(acc_r / total_point_size);
+    p.out_i[a * p.S + n] = from_f<T>(acc_i / total_point_size);
+  }
+}
+
+// MIXED forward.  Block = (antenna x point split, sample range).  Phase 1:
+// thread t forms the geometry of point p0 + t, culled and out-of-bounds
+// points are compacted away, and each surviving point stores its group seeds
+// amp exp(j phi(n_g)) and its per-sample rotator zeta.  Phase 2: thread
+// (group g, lane l) rotates the seeds of its lane's points through K samples.
+template <typename T, int K>
+__global__ void __launch_bounds__(256) tracer_fwd_mixed_kernel(const TrP<T> p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int TILE = blockDim.x;
+  const int G = p.groups;
+  const int L = blockDim.x / G;
+  float2* seeds = reinterpret_cast<float2*>(smem);        // [G][TILE]
+  float2* zeta = seeds + static_cast<size_t>(G) * TILE;   // [TILE]
+  int* warp_base = reinterpret_cast<int*>(zeta + TILE);   // [32]
+
+  const int64_t a = blockIdx.x / p.splits;
+  const int split = blockIdx.x % p.splits;
+  const int64_t n_begin = static_cast<int64_t>(blockIdx.y) * G * K;
+  const int64_t pt_begin = static_cast<int64_t>(split) * p.per_split;
+  const int64_t pt_end = min(p.P, pt_begin + p.per_split);
+
+  float txp[3], rxp[3];
+  load3(p.tx, a, txp);
+  load3(p.rx, a, rxp);
+  const double tx = txp[0], ty = txp[1], tz = txp[2], rx = rxp[0], ry = rxp[1], rz = rxp[2];
+
+  const int g = threadIdx.x / L;
+  const int l = threadIdx.x - g * L;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  float accr[K], acci[K], hir[K], hii[K];
+#pragma unroll
+  for (int m = 0; m < K; ++m) accr[m] = acci[m] = hir[m] = hii[m] = 0.0f;
+
+  for (int64_t p0 = pt_begin; p0 < pt_end; p0 += TILE) {
+    const int64_t pi = p0 + threadIdx.x;
+    bool valid = false;
+    float2 w = make_float2(0.0f, 0.0f), zt = make_float2(1.0f, 0.0f), zk = make_float2(1.0f, 0.0f);
+    if (pi < pt_end && p.inb[pi]) {
+      float nrm[3], pt[3];
+      load3(p.normals, pi, nrm);
+      load3(p.points, pi, pt);
+      SpecGeom geo;
+      specular_geometry(txp, rxp, nrm, pt, geo);
+      if (!culled(geo)) {
+        const float propagation_distance = path_distance(txp, rxp, pt);
+        const float amp = ld_f(p.sigmas, a * p.P + pi) * geo.align / sq(propagation_distance);
+        const double px = pt[0], py = pt[1], pz = pt[2];
+        const PhaseCycles pc =
+            path_cycles(tx - px, ty - py, tz - pz, rx - px, ry - py, rz - pz, p.k0, p.b0, p.k1, p.b1);
+        float start = pc.frac0;
+        if (n_begin != 0) {
+          const double c = static_cast<double>(pc.frac0) + static_cast<double>(n_begin) * pc.dcyc;
+          start = static_cast<float>(c - rint(c));
+        }
+        const float2 e = cis_cycles(start);
+        w = make_float2(amp * e.x, amp * e.y);
+        zt = cis_cycles(pc.dcyc);
+        const float kc = pc.dcyc * static_cast<float>(K);
+        zk = cis_cycles(kc - rintf(kc));
+        valid = true;
+      }
+    }
+    // Compact the surviving points of the tile.
+    const unsigned ballot = __ballot_sync(0xffffffffu, valid);
+    if (lane == 0) warp_base[warp] = __popc(ballot);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int run = 0;
+      for (int wi = 0; wi < nwarps; ++wi) {
+        const int c = warp_base[wi];
+        warp_base[wi] = run;
+        run += c;
+      }
+      warp_base[nwarps] = run;
+    }
+    __syncthreads();
+    const int count = warp_base[nwarps];
+    if (valid) {
+      const int slot = warp_base[warp] + __popc(ballot & ((1u << lane) - 1u));
+      zeta[slot] = zt;
+      for (int gg = 0; gg < G; ++gg) {
+        seeds[gg * TILE + slot] = w;
+        w = cmul(w, zk);
+      }
+    }
+    __syncthreads();
+    for (int vl = l; vl < count; vl += L) {
+      float2 s = seeds[g * TILE + vl];
+      const float2 z = zeta[vl];
+#pragma unroll
+      for (int m = 0; m < K; ++m) {
+        accr[m] += s.x;
+        acci[m] += s.y;
+        s = cmul(s, z);
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < K; ++m) {
+      hir[m] += accr[m];
+      hii[m] += acci[m];
+      accr[m] = acci[m] = 0.0f;
+    }
+    __syncthreads();
+  }
+
+  float2* red = reinterpret_cast<float2*>(smem);  // [G][K][L]
+#pragma unroll
+  for (int m = 0; m < K; ++m) red[(g * K + m) * L + l] = make_float2(hir[m], hii[m]);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < G * K; idx += blockDim.x) {
+    const int64_t n = n_begin + idx;
+    if (n >= p.S) continue;
+    float sr = 0.0f, si = 0.0f;
+    for (int ll = 0; ll < L; ++ll) {
+      const float2 v = red[idx * L + ll];
+      sr += v.x;
+      si += v.y;
+    }
+    if (p.splits == 1) {
+      p.out_r[a * p.S + n] = from_f<T>(sr / static_cast<float>(p.P));
+      p.out_i[a * p.S + n] = from_f<T>(si / static_cast<float>(p.P));
+    } else {
+      float* dst = p.partial + ((split * p.A + a) * p.S + n) * 2;
+      dst[0] = sr;
+      dst[1] = si;
+    }
+  }
+}
+
+template <typename T>
+__global__ void tracer_fwd_finalize_kernel(const float* __restrict__ partial, int splits,
+                                           int64_t count, float divisor, T* out_r, T* out_i) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < count;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double sr = 0.0, si = 0.0;
+    for (int s = 0; s < splits; ++s) {
+      sr += partial[(s * count + i) * 2 + 0];
+      si += partial[(s * count + i) * 2 + 1];
+    }
+    out_r[i] = from_f<T>(static_cast<float>(sr) / divisor);
+    out_i[i] = from_f<T>(static_cast<float>(si) / divisor);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint (point-major).  Block = point tile x antenna split; the residual
+// rows g[a, :] stream through a double-buffered TMA ring.
+struct AdjSmem {
+  size_t pos_off, buf_off, total;
+};
+
+template <typename T>
+AdjSmem adj_smem_layout(int rows, int ld) {
+  AdjSmem s;
+  s.pos_off = 128;
+  size_t off = s.pos_off + 2 * static_cast<size_t>(rows) * 6 * sizeof(float);
+  off = (off + 127) & ~static_cast<size_t>(127);
+  s.buf_off = off;
+  off += 4 * static_cast<size_t>(rows) * ld * sizeof(T);
+  s.total = (off + 127) & ~static_cast<size_t>(127);
+  return s;
+}
+
+template <typename T>
+__device__ __forceinline__ void stage_positions_f(float* pos, int stage, int rows_max, const T* tx,
+                                                  const T* rx, int64_t a0, int rws) {
+  for (int i = threadIdx.x; i < rws * 6; i += blockDim.x) {
+    const int r = i / 6;
+    const int c = i - r * 6;
+    const T* src = c < 3 ? tx : rx;
+    pos[(stage * rows_max + r) * 6 + c] = ld_f(src, (a0 + r) * 3 + (c % 3));
+  }
+}
+
+// Writes one point's accumulated normal / position gradients (or partials).
+template <typename T>
+__device__ __forceinline__ void store_point_grads(const TrP<T>& p, int split, int64_t pi,
+                                                  const float* gn, const float* gp, bool with_points) {
+  if (p.splits == 1) {
+    const int total_point_size = static_cast<int>(p.P);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) p.g_normals[pi * 3 + k] = from_f<T>(gn[k] / total_point_size);
+    if (with_points) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) p.g_points[pi * 3 + k] = from_f<T>(gp[k] / total_point_size);
+    }
+  } else {
+    float* dst = p.partial + (split * p.P + pi) * 6;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      dst[k] = gn[k];
+      dst[3 + k] = with_points ? gp[k] : 0.0f;
+    }
+  }
+}
+
+// PLAIN adjoint: thread = point, antennas and samples in the reference's order
+// (SignalTracer_cuda_kernel.cu:491-586).  With grad_points requested, the delay
+// derivative sum_n w_n (g_i cos - g_r sin) is accumulated alongside.
+template <typename T, bool WITH_POINTS>
+__global__ void __launch_bounds__(128) tracer_bwd_plain_kernel(const TrP<T> p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  float* pos = reinterpret_cast<float*>(smem + p.pos_off);
+  PairStager<T> stg{reinterpret_cast<T*>(smem + p.buf_off), bar, p.ld, p.rows, p.bulk != 0};
+
+  const int split = blockIdx.x % p.splits;
+  const int64_t ptile = blockIdx.x / p.splits;
+  const int64_t pi = ptile * blockDim.x + threadIdx.x;
+  const int64_t a_begin = static_cast<int64_t>(split) * p.per_split;
+  const int64_t a_end = min(p.A, a_begin + p.per_split);
+  const int ntiles = a_end > a_begin ? ceil_div(a_end - a_begin, p.rows) : 0;
+  const int S = static_cast<int>(p.S);
+  const bool inside = pi < p.P;
+  const bool active = inside && p.inb[pi];
+
+  if (p.bulk && threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  float nrm[3] = {0.0f, 0.0f, 0.0f}, pt[3] = {0.0f, 0.0f, 0.0f};
+  if (active) {
+    load3(p.normals, pi, nrm);
+    load3(p.points, pi, pt);
+  }
+  const float phase_base = p.phase_base;
+  const float phase_slope = p.phase_slope;
+  float accum_grad_normal[3] = {0.0f, 0.0f, 0.0f};
+  float accum_grad_point[3] = {0.0f, 0.0f, 0.0f};
+
+  auto issue = [&](int tile, int stage) {
+    const int64_t a0 = a_begin + static_cast<int64_t>(tile) * p.rows;
+    const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
+    stg.issue(stage, p.gr, p.gi, a0, rws, S);
+    stage_positions_f<T>(pos, stage, p.rows, p.tx, p.rx, a0, rws);
+  };
+  if (ntiles > 0) issue(0, 0);
+  if (ntiles > 1) issue(1, 1);
+
+  for (int t = 0; t < ntiles; ++t) {
+    const int s = t & 1;
+    if (!stg.wait(s, (t >> 1) & 1, p.status)) {
+      if (t + 1 < ntiles) stg.drain(s ^ 1, ((t + 1) >> 1) & 1, p.status);
+      return;
+    }
+    const int64_t a0 = a_begin + static_cast<int64_t>(t) * p.rows;
+    const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
+    for (int r = 0; r < rws && inside; ++r) {
+      const int64_t a = a0 + r;
+      if (!active) {
+        p.g_sigmas[a * p.P + pi] = from_f<T>(0.0f);
+        continue;
+      }
+      const float* ps = pos + (s * p.rows + r) * 6;
+      const float txp[3] = {ps[0], ps[1], ps[2]};
+      const float rxp[3] = {ps[3], ps[4], ps[5]};
+      SpecGeom g;
+      specular_geometry(txp, rxp, nrm, pt, g);
+      if (culled(g)) {
+        p.g_sigmas[a * p.P + pi] = from_f<T>(0.0f);
+        continue;
+      }
+      float gsa[3];
+      align_normal_gradient(g, nrm, gsa);
+      float propagation_distance = path_distance(txp, rxp, pt);
+      const float propagation_attenuation = 1.0f / sq(propagation_distance);
+      const float sigma_value = ld_f(p.sigmas, a * p.P + pi);
+      const float dist_path = propagation_distance;
+      propagation_distance += kPathBias;
+      const float tau = propagation_distance / kSpeedOfLight;
+      const T* rowr = stg.stage_ptr(s, 0) + r * p.ld;
+      const T* rowi = stg.stage_ptr(s, 1) + r * p.ld;
+      float accum_grad_sigma = 0.0f;
+      float accum_raw = 0.0f;
+      float accum_tau = 0.0f;
+      for (int n = 0; n < S; ++n) {
+        const float sample_time = static_cast<float>(n) / p.fs;
+        const float omega = phase_base + phase_slope * sample_time;
+        const float phase = omega * tau;
+        const float phase_real = cosf(phase);
+        const float phase_imag = sinf(phase);
+        const float gro = static_cast<float>(rowr[n]);
+        const float gio = static_cast<float>(rowi[n]);
+        const float grad_real = gro * phase_real;
+        const float grad_imag = gio * phase_imag;
+        const float normal_scale = sigma_value * propagation_attenuation;
+        accum_grad_normal[0] += normal_scale * gsa[0] * (grad_real + grad_imag);
+        accum_grad_normal[1] += normal_scale * gsa[1] * (grad_real + grad_imag);
+        accum_grad_normal[2] += normal_scale * gsa[2] * (grad_real + grad_imag);
+        accum_grad_sigma += propagation_attenuation * g.align * (grad_real + grad_imag);
+        if (WITH_POINTS) {
+          accum_raw += grad_real + grad_imag;
+          accum_tau += omega * (gio * phase_real - gro * phase_imag);
+        }
+      }
+      p.g_sigmas[a * p.P + pi] = from_f<T>(accum_grad_sigma / static_cast<int>(p.P));
+      if (WITH_POINTS) {
+        // dL/dp = dL/damp * damp/dp + dL/dtau * dtau/dp (before the 1/P factor)
+        const float amp = sigma_value * g.align * propagation_attenuation;
+        const float d_amp = accum_raw;
+        const float dist_t = sqrtf(sq(txp[0] - pt[0]) + sq(txp[1] - pt[1]) + sq(txp[2] - pt[2]));
+        const float dist_r = sqrtf(sq(rxp[0] - pt[0]) + sq(rxp[1] - pt[1]) + sq(rxp[2] - pt[2]));
+        float drho[3];
+        align_point_gradient(g, nrm, dist_t, dist_r, drho);
+        const float d_tau = amp * accum_tau;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const float dD = g.inc[k] - g.ret[k];
+          const float damp_dp =
+              sigma_value * propagation_attenuation * drho[k] - 2.0f * amp / dist_path * dD;
+          accum_grad_point[k] += d_amp * damp_dp + d_tau * dD / kSpeedOfLight;
+        }
+      }
+    }
+    __syncthreads();
+    if (t + 2 < ntiles) issue(t + 2, s);
+  }
+  if (inside) store_point_grads(p, split, pi, accum_grad_normal, accum_grad_point, WITH_POINTS);
+}
+
+// MIXED adjoint: thread = VPT points; per (point, antenna) the residual
+// polynomial Q(zeta) = sum_n conj(g[a,n]) zeta^n is evaluated by Horner
+// (4 FMA per sample) and, for position gradients, Q1 = sum_n n conj(g) zeta^n
+// alongside (4 more FMA per sample).
+template <typename T, bool WITH_POINTS>
+__global__ void __launch_bounds__(128) tracer_bwd_mixed_kernel(const TrP<T> p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  float* pos = reinterpret_cast<float*>(smem + p.pos_off);
+  PairStager<T> stg{reinterpret_cast<T*>(smem + p.buf_off), bar, p.ld, p.rows, p.bulk != 0};
+
+  const int split = blockIdx.x % p.splits;
+  const int64_t ptile = blockIdx.x / p.splits;
+  const int64_t pi = ptile * blockDim.x + threadIdx.x;
+  const int64_t a_begin = static_cast<int64_t>(split) * p.per_split;
+  const int64_t a_end = min(p.A, a_begin + p.per_split);
+  const int ntiles = a_end > a_begin ? ceil_div(a_end - a_begin, p.rows) : 0;
+  const bool inside = pi < p.P;
+  const bool active = inside && p.inb[pi];
+
+  if (p.bulk && threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  float nrm[3] = {0.0f, 0.0f, 1.0f}, pt[3] = {0.0f, 0.0f, 0.0f};
+  if (active) {
+    load3(p.normals, pi, nrm);
+    load3(p.points, pi, pt);
+  }
+  const double px = pt[0], py = pt[1], pz = pt[2];
+  // w0 and w1/fs in rad per unit delay, as exact FP64 products of the FP32 constants.
+  const float w0 = static_cast<float>(2.0 * static_cast<double>(kPiF) * p.f0);
+  const float w1s = static_cast<float>(2.0 * static_cast<double>(kPiF) * p.As / p.fs);
+  float gnorm[3] = {0.0f, 0.0f, 0.0f};
+  float gpt[3] = {0.0f, 0.0f, 0.0f};
+
+  auto issue = [&](int tile, int stage) {
+    const int64_t a0 = a_begin + static_cast<int64_t>(tile) * p.rows;
+    const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
+    stg.issue(stage, p.gr, p.gi, a0, rws, static_cast<int>(p.S));
+    stage_positions_f<T>(pos, stage, p.rows, p.tx, p.rx, a0, rws);
+  };
+  if (ntiles > 0) issue(0, 0);
+  if (ntiles > 1) issue(1, 1);
+
+  for (int t = 0; t < ntiles; ++t) {
+    const int s = t & 1;
+    if (!stg.wait(s, (t >> 1) & 1, p.status)) {
+      if (t + 1 < ntiles) stg.drain(s ^ 1, ((t + 1) >> 1) & 1, p.status);
+      return;
+    }
+    const int64_t a0 = a_begin + static_cast<int64_t>(t) * p.rows;
+    const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
+    for (int r = 0; r < rws && inside; ++r) {
+      const int64_t a = a0 + r;
+      const float* ps = pos + (s * p.rows + r) * 6;
+      const float txp[3] = {ps[0], ps[1], ps[2]};
+      const float rxp[3] = {ps[3], ps[4], ps[5]};
+      SpecGeom geo;
+      bool live = false;
+      if (active) {
+        specular_geometry(txp, rxp, nrm, pt, geo);
+        live = !culled(geo);
+      }
+      if (!live) {
+        p.g_sigmas[a * p.P + pi] = from_f<T>(0.0f);
+        continue;
+      }
+      const PhaseCycles pc = path_cycles(ps[0] - px, ps[1] - py, ps[2] - pz, ps[3] - px,
+                                         ps[4] - py, ps[5] - pz, p.k0, p.b0, p.k1, p.b1);
+      const float2 zt = cis_cycles(pc.dcyc);
+      const T* rowr = stg.stage_ptr(s, 0) + r * p.ld;
+      const T* rowi = stg.stage_ptr(s, 1) + r * p.ld;
+      // Horner with c_n = conj(g_n): q <- q zeta + c_n;  d <- d zeta + q (before q's update).
+      float qr = 0.0f, qi = 0.0f, dr = 0.0f, di = 0.0f;
+#pragma unroll 2
+      for (int n = p.ld - 4; n >= 0; n -= 4) {
+        const float4 a4 = lds4(rowr + n);
+        const float4 b4 = lds4(rowi + n);
+        const float cr[4] = {a4.w, a4.z, a4.y, a4.x};
+        const float cim[4] = {b4.w, b4.z, b4.y, b4.x};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (WITH_POINTS) {
+            const float ndr = fmaf(dr, zt.x, fmaf(-di, zt.y, qr));
+            const float ndi = fmaf(dr, zt.y, fmaf(di, zt.x, qi));
+            dr = ndr;
+            di = ndi;
+          }
+          const float nqr = fmaf(qr, zt.x, fmaf(-qi, zt.y, cr[q]));
+          const float nqi = fmaf(qr, zt.y, fmaf(qi, zt.x, -cim[q]));
+          qr = nqr;
+          qi = nqi;
+        }
+      }
+      const float2 e0 = cis_cycles(pc.frac0);
+      const float2 eq = cmul(e0, make_float2(qr, qi));
+      // sum_n (g_r cos + g_i sin) = Re(exp(j phi0) Q)
+      const float sum_re = eq.x;
+      const float propagation_distance = path_distance(txp, rxp, pt);
+      const float propagation_attenuation = 1.0f / sq(propagation_distance);
+      const float sigma_value = ld_f(p.sigmas, a * p.P + pi);
+      p.g_sigmas[a * p.P + pi] =
+          from_f<T>(propagation_attenuation * geo.align * sum_re / static_cast<float>(p.P));
+      float gsa[3];
+      align_normal_gradient(geo, nrm, gsa);
+      const float normal_scale = sigma_value * propagation_attenuation;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) gnorm[k] += normal_scale * gsa[k] * sum_re;
+      if (WITH_POINTS) {
+        // Q1 = zeta Q'(zeta);  sum_n w_n (g_i cos - g_r sin) = -Im(exp(j phi0) (w0 Q + w1s Q1))
+        const float2 q1 = cmul(zt, make_float2(dr, di));
+        const float2 f = cmul(e0, make_float2(w0 * qr + w1s * q1.x, w0 * qi + w1s * q1.y));
+        const float amp = sigma_value * geo.align * propagation_attenuation;
+        const float d_tau = -amp * f.y;
+        const float dist_t = sqrtf(sq(txp[0] - pt[0]) + sq(txp[1] - pt[1]) + sq(txp[2] - pt[2]));
+        const float dist_r = sqrtf(sq(rxp[0] - pt[0]) + sq(rxp[1] - pt[1]) + sq(rxp[2] - pt[2]));
+        float drho[3];
+        align_point_gradient(geo, nrm, dist_t, dist_r, drho);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const float dD = geo.inc[k] - geo.ret[k];
+          const float damp_dp =
+              normal_scale * drho[k] - 2.0f * amp / propagation_distance * dD;
+          gpt[k] += sum_re * damp_dp + d_tau * dD / kSpeedOfLight;
+        }
+      }
+    }
+    __syncthreads();
+    if (t + 2 < ntiles) issue(t + 2, s);
+  }
+  if (inside) store_point_grads(p, split, pi, gnorm, gpt, WITH_POINTS);
+}
+
+template <typename T>
+__global__ void tracer_bwd_finalize_kernel(const float* __restrict__ partial, int splits, int64_t P,
+                                           T* g_normals, T* g_points) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < P;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int s = 0; s < splits; ++s) {
+      const float* src = partial + (s * P + i) * 6;
+      for (int k = 0; k < 6; ++k) acc[k] += src[k];
+    }
+    const float inv = static_cast<float>(P);
+    for (int k = 0; k < 3; ++k) g_normals[i * 3 + k] = from_f<T>(static_cast<float>(acc[k]) / inv);
+    if (g_points != nullptr) {
+      for (int k = 0; k < 3; ++k) g_points[i * 3 + k] = from_f<T>(static_cast<float>(acc[3 + k]) / inv);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Along-ray linear resampler (SignalTracer_cuda_kernel.cu:199-349).  One warp
+// per ray: the bracketing index and weights of every target depth are found
+// once per ray (binary search over the ray's coarse depths) and reused for all
+// A sigma rows; arithmetic is in the element type, as in the reference.
+template <typename T>
+struct BiP {
+  const T* normals;
+  const T* sigmas;
+  const T* z;
+  const T* tz;
+  T* out_n;
+  T* out_s;
+  uint8_t* out_inb;
+  int64_t A, R, S, T_;
+};
+
+template <typename T>
+__device__ __forceinline__ int bracket_lower(const T* z, int S, T target) {
+  int lower_index = 0;
+  int upper_index = S - 1;
+  while (lower_index < upper_index - 1) {
+    const int mid_index = (lower_index + upper_index) / 2;
+    if (z[mid_index] <= target) lower_index = mid_index;
+    else upper_index = mid_index;
+  }
+  return lower_index;
+}
+
+template <typename T>
+__device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
+
+// acc + w * g with the product rounded before the sum (never fused), as an
+// atomicAdd of a precomputed product does in the reference.
+__device__ __forceinline__ float add_product(float acc, float w, float g) {
+  return __fadd_rn(acc, __fmul_rn(w, g));
+}
+__device__ __forceinline__ double add_product(double acc, double w, double g) {
+  return __dadd_rn(acc, __dmul_rn(w, g));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) bilinear_fwd_kernel(const BiP<T> p) {
+  const int64_t ray = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (ray >= p.R) return;
+  const int S = static_cast<int>(p.S);
+  const T* z = p.z + ray * p.S;
+  const T* nrm = p.normals + ray * p.S * 3;
+  for (int64_t t = lane; t < p.T_; t += 32) {
+    const T target = p.tz[ray * p.T_ + t];
+    const int lo = bracket_lower(z, S, target);
+    const T z0 = z[lo];
+    const T z1 = z[lo + 1];
+    const bool oob = (target < z0) || (target > z1);
+    p.out_inb[ray * p.T_ + t] = oob ? 0 : 1;
+    T* on = p.out_n + (ray * p.T_ + t) * 3;
+    if (oob) {
+      on[0] = T(0.0f);
+      on[1] = T(0.0f);
+      on[2] = T(0.0f);
+      for (int64_t a = 0; a < p.A; ++a) p.out_s[(a * p.R + ray) * p.T_ + t] = T(0.0f);
+      continue;
+    }
+    const T weight_upper = (target - z0) / tmax(z1 - z0, static_cast<T>(1.0e-6f));
+    const T weight_lower = static_cast<T>(1) - weight_upper;
+    for (int axis = 0; axis < 3; ++axis) {
+      const T normal_lower = nrm[lo * 3 + axis];
+      const T normal_upper = nrm[(lo + 1) * 3 + axis];
+      on[axis] = weight_lower * normal_lower + weight_upper * normal_upper;
+    }
+    for (int64_t a = 0; a < p.A; ++a) {
+      const T* sg = p.sigmas + (a * p.R + ray) * p.S;
+      p.out_s[(a * p.R + ray) * p.T_ + t] = weight_lower * sg[lo] + weight_upper * sg[lo + 1];
+    }
+  }
+}
+
+// Adjoint, gather form: lane j of the ray's warp owns coarse sample j and adds
+// the contributions of the targets bracketing it in target order -- the same
+// per-element order as the reference's single-writer atomicAdd sequence --
+// onto the existing gradient value.
+template <typename T>
+__global__ void __launch_bounds__(256) bilinear_bwd_kernel(const BiP<T> p) {
+  const int64_t ray = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (ray >= p.R) return;
+  const int S = static_cast<int>(p.S);
+  const T* z = p.z + ray * p.S;
+  // p.normals = grad_output_normals [R,T,3], p.sigmas = grad_output_sigmas [A,R,T]
+  for (int j = lane; j < S; j += 32) {
+    T gn[3] = {p.out_n[(ray * p.S + j) * 3 + 0], p.out_n[(ray * p.S + j) * 3 + 1],
+               p.out_n[(ray * p.S + j) * 3 + 2]};
+    for (int64_t t = 0; t < p.T_; ++t) {
+      const T target = p.tz[ray * p.T_ + t];
+      const int lo = bracket_lower(z, S, target);
+      if (lo != j && lo + 1 != j) continue;
+      const T z0 = z[lo];
+      const T z1 = z[lo + 1];
+      if (target < z0 || target > z1) continue;
+      const T weight_upper = (target - z0) / tmax(z1 - z0, static_cast<T>(1.0e-6f));
+      const T weight_lower = static_cast<T>(1) - weight_upper;
+      const T* gno = p.normals + (ray * p.T_ + t) * 3;
+      for (int axis = 0; axis < 3; ++axis) {
+        if (lo == j) gn[axis] = add_product(gn[axis], weight_lower, gno[axis]);
+        if (lo + 1 == j) gn[axis] = add_product(gn[axis], weight_upper, gno[axis]);
+      }
+    }
+    for (int axis = 0; axis < 3; ++axis) p.out_n[(ray * p.S + j) * 3 + axis] = gn[axis];
+  }
+  for (int64_t a = 0; a < p.A; ++a) {
+    const T* gso = p.sigmas + (a * p.R + ray) * p.T_;
+    T* gs = p.out_s + (a * p.R + ray) * p.S;
+    for (int j = lane; j < S; j += 32) {
+      T acc = gs[j];
+      for (int64_t t = 0; t < p.T_; ++t) {
+        const T target = p.tz[ray * p.T_ + t];
+        const int lo = bracket_lower(z, S, target);
+        if (lo != j && lo + 1 != j) continue;
+        const T z0 = z[lo];
+        const T z1 = z[lo + 1];
+        if (target < z0 || target > z1) continue;
+        const T weight_upper = (target - z0) / tmax(z1 - z0, static_cast<T>(1.0e-6f));
+        const T weight_lower = static_cast<T>(1) - weight_upper;
+        if (lo == j) acc = add_product(acc, weight_lower, gso[t]);
+        if (lo + 1 == j) acc = add_product(acc, weight_upper, gso[t]);
+      }
+      gs[j] = acc;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+bool aligned16(const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; }
+
+template <typename T>
+TrP<T> make_params(const TracerArgs& a) {
+  TrP<T> p;
+  p.normals = static_cast<const T*>(a.normals);
+  p.sigmas = static_cast<const T*>(a.sigmas);
+  p.points = static_cast<const T*>(a.points);
+  p.tx = static_cast<const T*>(a.tx);
+  p.rx = static_cast<const T*>(a.rx);
+  p.inb = a.inbounds;
+  p.out_r = static_cast<T*>(a.out_real);
+  p.out_i = static_cast<T*>(a.out_imag);
+  p.gr = static_cast<const T*>(a.grad_real_out);
+  p.gi = static_cast<const T*>(a.grad_imag_out);
+  p.g_normals = static_cast<T*>(a.grad_normals);
+  p.g_sigmas = static_cast<T*>(a.grad_sigmas);
+  p.g_points = static_cast<T*>(a.grad_points);
+  p.partial = nullptr;
+  p.status = device_status_ptr();
+  p.A = a.A;
+  p.S = a.S;
+  p.P = a.P;
+  p.fs = a.fs;
+  p.f0 = a.f0;
+  p.As = a.As;
+  // The reference forms these per thread as 2.0f * kPi * start_frequency and
+  // 2.0f * kPi * chirp_slope_scaled (FP32).
+  p.phase_base = 2.0f * kPiF * a.f0;
+  p.phase_slope = 2.0f * kPiF * a.As;
+  const PhaseConsts pc = phase_consts(a.f0, a.As, a.fs);
+  p.k0 = pc.k0;
+  p.b0 = pc.b0;
+  p.k1 = pc.k1;
+  p.b1 = pc.b1;
+  p.splits = 1;
+  p.per_split = 0;
+  p.groups = 1;
+  p.rows = 1;
+  p.ld = 4;
+  p.bulk = 0;
+  p.pos_off = p.buf_off = 0;
+  return p;
+}
+
+// Sample groups per block (power of two, at most 64: shared-memory bound).
+int fwd_groups(int64_t S, int chunk, int threads) {
+  const int64_t g = (S + chunk - 1) / chunk;
+  int groups = 1;
+  while (groups < g && groups < threads && groups < 64) groups *= 2;
+  return groups;
+}
+
+template <typename T, int K>
+cudaError_t launch_tr_fwd_mixed_k(const TrP<T>& p, dim3 grid, int threads, size_t smem,
+                                  cudaStream_t st) {
+  const void* fn = reinterpret_cast<const void*>(&tracer_fwd_mixed_kernel<T, K>);
+  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+  if (err != cudaSuccess) return err;
+  void* args[] = {const_cast<TrP<T>*>(&p)};
+  return cudaLaunchKernel(fn, grid, dim3(threads), args, smem, st);
+}
+
+size_t fwd_mixed_smem(int threads, int groups, int chunk) {
+  const size_t seeds = (static_cast<size_t>(groups) + 1) * threads * sizeof(float2) + 33 * sizeof(int);
+  const size_t red = static_cast<size_t>(threads) * chunk * sizeof(float2);
+  return std::max(seeds, red);
+}
+
+template <typename T>
+cudaError_t launch_tracer_fwd(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  TrP<T> p = make_params<T>(a);
+  p.partial = static_cast<float*>(ws);
+  if (a.mode == kPlain) {
+    const int threads = 128;
+    dim3 grid(static_cast<unsigned>(a.A), static_cast<unsigned>((a.S + threads - 1) / threads));
+    tracer_fwd_plain_kernel<T><<<grid, threads, 0, st>>>(p);
+    return cudaGetLastError();
+  }
+  const int threads = t.threads;
+  const int chunk = t.chunk;
+  const int groups = fwd_groups(a.S, chunk, threads);
+  p.groups = groups;
+  p.splits = t.splits;
+  p.per_split = (a.P + t.splits - 1) / t.splits;
+  const int64_t ranges = (a.S + static_cast<int64_t>(groups) * chunk - 1) /
+                         (static_cast<int64_t>(groups) * chunk);
+  dim3 grid(static_cast<unsigned>(a.A * t.splits), static_cast<unsigned>(ranges));
+  const size_t smem = fwd_mixed_smem(threads, groups, chunk);
+  cudaError_t err;
+  if (chunk == 8) err = launch_tr_fwd_mixed_k<T, 8>(p, grid, threads, smem, st);
+  else if (chunk == 32) err = launch_tr_fwd_mixed_k<T, 32>(p, grid, threads, smem, st);
+  else err = launch_tr_fwd_mixed_k<T, 16>(p, grid, threads, smem, st);
+  if (err != cudaSuccess) return err;
+  if (t.splits > 1) {
+    const int64_t count = a.A * a.S;
+    const int fin_blocks = static_cast<int>(std::min<int64_t>((count + 255) / 256, 148 * 16));
+    tracer_fwd_finalize_kernel<T><<<std::max(fin_blocks, 1), 256, 0, st>>>(
+        p.partial, t.splits, count, static_cast<float>(a.P), p.out_r, p.out_i);
+    err = cudaGetLastError();
+  }
+  return err;
+}
+
+template <typename T>
+cudaError_t launch_tracer_bwd(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  TrP<T> p = make_params<T>(a);
+  p.partial = static_cast<float*>(ws);
+  const int threads = t.threads;
+  p.splits = t.splits;
+  const int64_t rows_total = std::max<int64_t>(1, (a.A + t.stage_rows - 1) / t.stage_rows);
+  p.per_split = ((rows_total + t.splits - 1) / t.splits) * t.stage_rows;
+  p.ld = static_cast<int>(((std::max<int64_t>(a.S, 1) + 3) / 4) * 4);
+  const size_t es = a.dtype == kF64 ? 8 : 4;
+  p.bulk = (a.S > 0 && a.S % 4 == 0 && (a.S * es) % 16 == 0 && aligned16(a.grad_real_out) &&
+            aligned16(a.grad_imag_out))
+               ? 1
+               : 0;
+  int rows = t.stage_rows;
+  AdjSmem lay = adj_smem_layout<T>(rows, p.ld);
+  const DeviceInfo dev = current_device_info();
+  while (rows > 1 && lay.total > static_cast<size_t>(dev.max_smem_optin)) {
+    rows /= 2;
+    lay = adj_smem_layout<T>(rows, p.ld);
+  }
+  if (rows != t.stage_rows) {
+    p.per_split = ((std::max<int64_t>(1, (a.A + rows - 1) / rows) + t.splits - 1) / t.splits) * rows;
+  }
+  p.rows = rows;
+  p.pos_off = lay.pos_off;
+  p.buf_off = lay.buf_off;
+  const bool with_points = a.grad_points != nullptr;
+  const void* fn;
+  if (a.mode == kPlain) {
+    fn = with_points ? reinterpret_cast<const void*>(&tracer_bwd_plain_kernel<T, true>)
+                     : reinterpret_cast<const void*>(&tracer_bwd_plain_kernel<T, false>);
+  } else {
+    fn = with_points ? reinterpret_cast<const void*>(&tracer_bwd_mixed_kernel<T, true>)
+                     : reinterpret_cast<const void*>(&tracer_bwd_mixed_kernel<T, false>);
+  }
+  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(lay.total));
+  if (err != cudaSuccess) return err;
+  const int64_t ptiles = (a.P + threads - 1) / threads;
+  const int64_t blocks = ptiles * t.splits;
+  if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
+  void* args[] = {&p};
+  err = cudaLaunchKernel(fn, dim3(static_cast<unsigned>(blocks)), dim3(threads), args, lay.total, st);
+  if (err != cudaSuccess) return err;
+  if (t.splits > 1) {
+    const int fin_blocks = static_cast<int>(std::min<int64_t>((a.P + 255) / 256, 148 * 16));
+    tracer_bwd_finalize_kernel<T><<<std::max(fin_blocks, 1), 256, 0, st>>>(
+        p.partial, t.splits, a.P, p.g_normals, with_points ? p.g_points : nullptr);
+    err = cudaGetLastError();
+  }
+  return err;
+}
+
+template <typename T>
+BiP<T> make_bi(const BilinearArgs& a) {
+  BiP<T> p;
+  p.normals = static_cast<const T*>(a.normals);
+  p.sigmas = static_cast<const T*>(a.sigmas);
+  p.z = static_cast<const T*>(a.z_vals);
+  p.tz = static_cast<const T*>(a.tz_vals);
+  p.out_n = static_cast<T*>(a.out_normals);
+  p.out_s = static_cast<T*>(a.out_sigmas);
+  p.out_inb = a.out_inbounds;
+  p.A = a.A;
+  p.R = a.R;
+  p.S = a.S;
+  p.T_ = a.T;
+  return p;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+Tuning tracer_forward_resolve(const TracerArgs& a, const Tuning& req) {
+  Tuning t = req;
+  if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 256;
+  if (t.chunk != 8 && t.chunk != 16 && t.chunk != 32) t.chunk = 16;
+  if (t.items <= 0) t.items = 1;
+  if (t.stage_rows <= 0) t.stage_rows = 8;
+  if (a.mode == kPlain) {
+    t.splits = 1;
+    return t;
+  }
+  const int groups = fwd_groups(a.S, t.chunk, t.threads);
+  const int64_t ranges = (a.S + static_cast<int64_t>(groups) * t.chunk - 1) /
+                         (static_cast<int64_t>(groups) * t.chunk);
+  const int64_t ptiles = std::max<int64_t>(1, (a.P + t.threads - 1) / t.threads);
+  if (t.splits <= 0) {
+    const DeviceInfo dev = current_device_info();
+    const int per_sm = std::max(1, 512 / t.threads);
+    t.splits = pick_splits(std::max<int64_t>(1, a.A * ranges), per_sm, dev.sm_count, ptiles);
+  }
+  t.splits = static_cast<int>(std::min<int64_t>(std::max(t.splits, 1), ptiles));
+  return t;
+}
+
+size_t tracer_forward_workspace(const TracerArgs& a, const Tuning& t) {
+  if (a.mode == kPlain || t.splits <= 1) return 0;
+  return static_cast<size_t>(t.splits) * a.A * a.S * 2 * sizeof(float);
+}
+
+cudaError_t tracer_forward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  if (a.A == 0 || a.S == 0) return cudaSuccess;
+  if (a.dtype == kF64) return launch_tracer_fwd<double>(a, t, ws, st);
+  return launch_tracer_fwd<float>(a, t, ws, st);
+}
+
+Tuning tracer_backward_resolve(const TracerArgs& a, const Tuning& req) {
+  Tuning t = req;
+  if (t.threads != 64 && t.threads != 128) t.threads = 128;
+  if (t.items <= 0) t.items = 1;
+  if (t.stage_rows <= 0) t.stage_rows = 8;
+  t.stage_rows = std::min(t.stage_rows, 64);
+  if (t.chunk <= 0) t.chunk = 16;
+  const int64_t rows_total = std::max<int64_t>(1, (a.A + t.stage_rows - 1) / t.stage_rows);
+  if (t.splits <= 0) {
+    const int64_t ptiles = std::max<int64_t>(1, (a.P + t.threads - 1) / t.threads);
+    const DeviceInfo dev = current_device_info();
+    const int per_sm = std::max(1, 1024 / t.threads);
+    t.splits = a.mode == kPlain ? 1 : pick_splits(ptiles, per_sm, dev.sm_count, rows_total);
+  }
+  t.splits = static_cast<int>(std::min<int64_t>(std::max(t.splits, 1), rows_total));
+  return t;
+}
+
+size_t tracer_backward_workspace(const TracerArgs& a, const Tuning& t) {
+  if (t.splits <= 1 || a.P == 0) return 0;
+  return static_cast<size_t>(t.splits) * a.P * 6 * sizeof(float);
+}
+
+cudaError_t tracer_backward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  if (a.P == 0) return cudaSuccess;
+  if (a.dtype == kF64) return launch_tracer_bwd<double>(a, t, ws, st);
+  return launch_tracer_bwd<float>(a, t, ws, st);
+}
+
+cudaError_t bilinear_forward(const BilinearArgs& a, cudaStream_t st) {
+  if (a.R == 0 || a.T == 0) return cudaSuccess;
+  const int64_t blocks = (a.R * 32 + 255) / 256;
+  if (a.dtype == kF64) bilinear_fwd_kernel<double><<<static_cast<unsigned>(blocks), 256, 0, st>>>(make_bi<double>(a));
+  else bilinear_fwd_kernel<float><<<static_cast<unsigned>(blocks), 256, 0, st>>>(make_bi<float>(a));
+  return cudaGetLastError();
+}
+
+cudaError_t bilinear_backward(const BilinearArgs& a, cudaStream_t st) {
+  if (a.R == 0 || a.S == 0) return cudaSuccess;
+  const int64_t blocks = (a.R * 32 + 255) / 256;
+  if (a.dtype == kF64) bilinear_bwd_kernel<double><<<static_cast<unsigned>(blocks), 256, 0, st>>>(make_bi<double>(a));
+  else bilinear_bwd_kernel<float><<<static_cast<unsigned>(blocks), 256, 0, st>>>(make_bi<float>(a));
+  return cudaGetLastError();
+}
+
+}  // namespace geraf

@@ -1,0 +1,213 @@
+/*
+ * geraf_rf.h -- C ABI of the B200 (sm_100a) RF operator library `libgeraf_rf.so`.
+ *
+ * The library implements GeRaF's two RF operators, the FMCW matched-filter
+ * backprojection (RFMatchedFilter) and the lensless specular signal tracer
+ * (RFSignalTracer), plus the along-ray resampler that ships in the same
+ * extension.  Every entry point here replaces one function of the reference's
+ * pybind `_C` modules; the reference file:line of that function is given above
+ * each declaration.  Paths are relative to the GeRaF-SENS checkout.
+ *
+ * Conventions (the same as the reference's `_C` functions):
+ *   - All tensor arguments are raw DEVICE pointers to contiguous row-major
+ *     arrays owned by the caller; outputs are written in place ("out-parameter"
+ *     style); nothing is allocated by the library.
+ *   - `dtype` selects the element type of every floating-point array of the
+ *     call (GERAF_DTYPE_*).  Boolean masks are one byte per element (0 / 1).
+ *   - Work is enqueued on `stream` (a cudaStream_t; NULL = legacy default
+ *     stream) and the call returns without synchronising.
+ *   - Return value: GERAF_OK, or a GERAF_ERR_* code; `geraf_rf_last_error()`
+ *     then holds a message for the calling thread.
+ *   - Entry points that may use a reduction workspace take `workspace` /
+ *     `workspace_bytes`; the matching `*_workspace_bytes` query returns the
+ *     size needed for the same arguments (0 when none is needed, in which case
+ *     `workspace` may be NULL).  A workspace must be 256-byte aligned device
+ *     memory and must not be shared by calls that may overlap on the GPU.
+ */
+#ifndef GERAF_RF_H_
+#define GERAF_RF_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GERAF_OK 0
+#define GERAF_ERR_INVALID_ARGUMENT 1 /* shape / size / pointer / dtype problem   */
+#define GERAF_ERR_UNSUPPORTED 2      /* valid request this build does not serve  */
+#define GERAF_ERR_WORKSPACE 3        /* workspace missing, short or misaligned   */
+#define GERAF_ERR_CUDA 4             /* a CUDA runtime call or launch failed      */
+#define GERAF_ERR_DEVICE_TIMEOUT 5   /* a bounded device-side wait gave up        */
+
+/* ---- element types (match the reference's AT_DISPATCH lists) ----------- */
+#define GERAF_DTYPE_F32 0
+#define GERAF_DTYPE_F64 1
+#define GERAF_DTYPE_F16 2 /* matched filter only, as in the reference */
+
+/* ---- arithmetic forms -------------------------------------------------- */
+/* PLAIN: the reference's FP32 arithmetic, expression for expression: one
+ *        accurate sinf/cosf per (voxel|point, antenna, sample) and the
+ *        reference's summation order per output element.  Judged against the
+ *        reference kernels (relative L2 <= 1e-5).
+ * MIXED: carrier phase f0*tau reduced modulo one cycle in FP64, per-sample
+ *        phasors by an FP32 Horner / rotator recurrence (2 phasors per
+ *        (voxel|point, antenna) instead of one per sample), compensated
+ *        (Kahan) accumulation across antennas.  Judged against an FP64 oracle
+ *        (relative L2 <= 1e-4).                                              */
+#define GERAF_MODE_PLAIN 0
+#define GERAF_MODE_MIXED 1
+
+/* Launch shape.  Any field left 0 takes the library default for the call. */
+typedef struct geraf_tuning {
+  int32_t threads;          /* threads per block: 64, 128 or 256                       */
+  int32_t items_per_thread; /* voxels (MF forward) or points (tracer adjoint): 1, 2, 4 */
+  int32_t stage_rows;       /* antenna rows per shared-memory stage                     */
+  int32_t splits;           /* partial-sum splits of the reduced dimension              */
+  int32_t chunk;            /* samples per lane in the sample-major kernels: 8,16,32    */
+} geraf_tuning_t;
+
+/* ---- library information ---------------------------------------------- */
+/* Message of the last failed call on this thread ("" if none). */
+const char* geraf_rf_last_error(void);
+/* CUDART_VERSION the library was built with (reference: csrc/cuda_version.cu:8). */
+int32_t geraf_rf_cudart_version(void);
+/* Compiler and target description, e.g. "GCC 13.3; nvcc 12.9; sm_100a"
+ * (reference: csrc/vision.cpp:47-68, get_compiler_version). */
+const char* geraf_rf_build_info(void);
+/* Measures nothing itself: enqueues blocks x threads threads (threads <= 256)
+ * of `iters` iterations of 8 independent FP32 FMAs, i.e. blocks*threads*iters*16
+ * flops, for timing by the caller.  `sink` is device memory of blocks*threads
+ * floats (never written in practice).  The FP32-pipe roofline denominator of
+ * the RF kernels; no counterpart in the reference. */
+int32_t geraf_rf_fma_probe(int32_t blocks, int32_t threads, int32_t iters, float* sink,
+                           void* stream);
+/* Reads, and with reset != 0 clears, the device status word of the current
+ * device (GERAF_OK or GERAF_ERR_DEVICE_TIMEOUT raised by a bounded wait inside
+ * a kernel).  Synchronises `stream`. */
+int32_t geraf_rf_device_status(void* stream, int32_t reset, int32_t* status_out);
+
+/* ---- RFMatchedFilter ---------------------------------------------------- */
+/* y[v] = (1/A) sum_a sum_n (re + j im)[a,n] * exp(-j phi(a,v,n)),
+ * phi = 2*pi*773.704*tau + 2*pi*As*(n/fs)*tau,  tau = (|tx_a-v| + |rx_a-v| + 0.15)/2.9979.
+ * real, imag: [A,S]; tx_pos, rx_pos: [A,3]; voxel: [3,N] (x row, y row, z row);
+ * output_real, output_imag: [N].
+ * Replaces MatchedFilter::MatchedFilter_forward
+ * (geraf/ops/RFMatchedFilter/csrc/matched_filter/MatchedFilter_cuda.cu:173-210,
+ *  kernel MatchedFilter_cuda_kernel.cu:65-115). */
+int32_t geraf_mf_forward_workspace_bytes(int64_t total_ant_size, int64_t num_adc_samples,
+                                         int64_t num_voxels, int32_t dtype, int32_t mode,
+                                         const geraf_tuning_t* tuning, size_t* bytes);
+int32_t geraf_mf_forward(const void* real, const void* imag, const void* tx_pos,
+                         const void* rx_pos, void* output_real, void* output_imag,
+                         const void* voxel, int64_t total_ant_size, int64_t num_adc_samples,
+                         float adc_sample_rate, float chirp_slope_scaled, int64_t num_voxels,
+                         int32_t dtype, int32_t mode, const geraf_tuning_t* tuning,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
+/* Exact adjoint of geraf_mf_forward with respect to (real, imag):
+ * grad[a,n] = (1/A) sum_v (g_r + j g_i)[v] * exp(+j phi(a,v,n)).
+ * grad_output_real/imag: [N]; grad_real, grad_imag: [A,S] (overwritten).
+ * `real`/`imag` are accepted for signature parity and not read.
+ * Replaces MatchedFilter::MatchedFilter_backward_realimag
+ * (MatchedFilter_cuda.cu:253-297, kernel MatchedFilter_cuda_kernel.cu:171-220). */
+int32_t geraf_mf_backward_workspace_bytes(int64_t total_ant_size, int64_t num_adc_samples,
+                                          int64_t num_voxels, int32_t dtype, int32_t mode,
+                                          const geraf_tuning_t* tuning, size_t* bytes);
+int32_t geraf_mf_backward(const void* grad_output_real, const void* grad_output_imag,
+                          const void* real, const void* imag, const void* tx_pos,
+                          const void* rx_pos, void* grad_real, void* grad_imag,
+                          const void* voxel, int64_t total_ant_size, int64_t num_adc_samples,
+                          float adc_sample_rate, float chirp_slope_scaled, int64_t num_voxels,
+                          int32_t dtype, int32_t mode, const geraf_tuning_t* tuning,
+                          void* workspace, size_t workspace_bytes, void* stream);
+
+/* Range-bin variant: per antenna, gather bin floor(d/fft_spacing/2) of the
+ * [A,bins] spectrum (skipped when d > fft_spacing*bins) times exp(-j 2 pi 773.704 tau).
+ * Replaces MatchedFilter::MatchedFilter_fft_forward (MatchedFilter_cuda.cu:212-251,
+ * kernel MatchedFilter_cuda_kernel.cu:117-169). */
+int32_t geraf_mf_fft_forward(const void* real, const void* imag, const void* tx_pos,
+                             const void* rx_pos, void* output_real, void* output_imag,
+                             const void* voxel, int64_t total_ant_size, int64_t num_range_bins,
+                             float fft_spacing, float adc_sample_rate, float chirp_slope_scaled,
+                             int64_t num_voxels, int32_t dtype, void* stream);
+/* Adjoint of geraf_mf_fft_forward.  Replaces
+ * MatchedFilter::MatchedFilter_fft_backward_realimag (MatchedFilter_cuda.cu:299-343,
+ * kernel MatchedFilter_cuda_kernel.cu:222-279). */
+int32_t geraf_mf_fft_backward(const void* grad_output_real, const void* grad_output_imag,
+                              const void* real, const void* imag, const void* tx_pos,
+                              const void* rx_pos, void* grad_real, void* grad_imag,
+                              const void* voxel, int64_t total_ant_size, int64_t num_range_bins,
+                              float fft_spacing, float adc_sample_rate, float chirp_slope_scaled,
+                              int64_t num_voxels, int32_t dtype, void* stream);
+
+/* ---- RFSignalTracer ----------------------------------------------------- */
+/* x[a,n] = (1/P) sum_{p in-bounds, not culled} sigma[a,p] * rho / D^2 * exp(+j (2 pi f0 + 2 pi As t_n) tau),
+ * rho = <normalize(rx_a - p), normalize(i - 2 (i.n) n)>, i = normalize(p - tx_a),
+ * culled when rho < 1e-6 or i.n > 0; D = |tx_a - p| + |rx_a - p|; tau = (D + 0.15)/2.9979.
+ * normals, points: [P,3]; sigmas: [A,P]; tx_pos, rx_pos: [A,3]; inbounds: [P] (u8);
+ * output_real, output_imag: [A,S].
+ * Replaces SignalTracer::SignalTracer_forward
+ * (geraf/ops/RFSignalTracer/csrc/signal_tracer/SignalTracer_cuda.cu:314-356,
+ *  kernel SignalTracer_cuda_kernel.cu:351-450). */
+int32_t geraf_tracer_forward_workspace_bytes(int64_t total_ant_size, int64_t num_adc_samples,
+                                             int64_t total_point_size, int32_t dtype, int32_t mode,
+                                             const geraf_tuning_t* tuning, size_t* bytes);
+int32_t geraf_tracer_forward(const void* normals, const void* sigmas, const void* points,
+                             const void* tx_pos, const void* rx_pos, const uint8_t* inbounds,
+                             void* output_real, void* output_imag, int64_t num_adc_samples,
+                             float adc_sample_rate, float start_frequency,
+                             float chirp_slope_scaled, int64_t total_ant_size,
+                             int64_t total_point_size, int32_t dtype, int32_t mode,
+                             const geraf_tuning_t* tuning, void* workspace,
+                             size_t workspace_bytes, void* stream);
+
+/* Adjoint of geraf_tracer_forward: grad_sigmas [A,P], grad_normals [P,3] and,
+ * when grad_points != NULL, grad_points [P,3] (the reference has no position
+ * gradient).  Entries of out-of-bounds points are written as zero (the
+ * reference leaves them unwritten).  grad_output_real/imag: [A,S].
+ * Replaces SignalTracer::SignalTracer_backward_normal_sigma
+ * (SignalTracer_cuda.cu:358-406, kernel SignalTracer_cuda_kernel.cu:452-587). */
+int32_t geraf_tracer_backward_workspace_bytes(int64_t total_ant_size, int64_t num_adc_samples,
+                                              int64_t total_point_size, int32_t dtype,
+                                              int32_t mode, int32_t with_points,
+                                              const geraf_tuning_t* tuning, size_t* bytes);
+int32_t geraf_tracer_backward(const void* grad_output_real, const void* grad_output_imag,
+                              const void* normals, const void* sigmas, const void* points,
+                              const void* tx_pos, const void* rx_pos, const uint8_t* inbounds,
+                              void* grad_normals, void* grad_sigmas, void* grad_points,
+                              int64_t num_adc_samples, float adc_sample_rate,
+                              float start_frequency, float chirp_slope_scaled,
+                              int64_t total_ant_size, int64_t total_point_size, int32_t dtype,
+                              int32_t mode, const geraf_tuning_t* tuning, void* workspace,
+                              size_t workspace_bytes, void* stream);
+
+/* Linear resampling along rays: for each ray and target depth, bracket the
+ * target in the ray's coarse depths by binary search and interpolate sigma
+ * (all A rows) and normals; out-of-range targets give 0 and inbounds = 0.
+ * normals [R,S,3], sigmas [A,R,S], z_vals [R,S], target_z_vals [R,T];
+ * output_normals [R,T,3], output_sigmas [A,R,T], output_inbounds [R,T] (u8).
+ * Replaces SignalTracer::BilinearRaysample_forward
+ * (SignalTracer_cuda.cu:241-276, kernel SignalTracer_cuda_kernel.cu:199-279). */
+int32_t geraf_bilinear_forward(const void* normals, const void* sigmas, const void* z_vals,
+                               const void* target_z_vals, void* output_normals,
+                               void* output_sigmas, uint8_t* output_inbounds,
+                               int64_t num_antennas, int64_t num_rays, int64_t num_samples,
+                               int64_t num_target_samples, int32_t dtype, void* stream);
+/* Adjoint of geraf_bilinear_forward; ADDS into grad_normals [R,S,3] and
+ * grad_sigmas [A,R,S] (the reference's callers pass zeroed buffers).
+ * Replaces SignalTracer::BilinearRaysample_backward
+ * (SignalTracer_cuda.cu:278-312, kernel SignalTracer_cuda_kernel.cu:281-349). */
+int32_t geraf_bilinear_backward(const void* grad_output_normals, const void* grad_output_sigmas,
+                                const void* z_vals, const void* target_z_vals,
+                                void* grad_normals, void* grad_sigmas, int64_t num_antennas,
+                                int64_t num_rays, int64_t num_samples,
+                                int64_t num_target_samples, int32_t dtype, void* stream);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* GERAF_RF_H_ */

@@ -1,0 +1,183 @@
+"""numpy interface of the CPU oracle (``oracle/rf_oracle.c``).
+
+TEST INFRASTRUCTURE ONLY -- imported by tests/, by ``__graft_entry__.smoke()``
+as the checker and by ``bench.py``'s CPU-baseline leg; never by the product.
+
+Every function takes FP32 numpy arrays in the reference's layouts (voxels as
+[3, N]) and returns new arrays: ``*_f64`` functions return float64 results of
+the exact-arithmetic model, ``*_f32`` functions float32 results of the
+reference's FP32 operation order.  Which reference lines each follows is
+stated in ``rf_oracle.c``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+_lib = None
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_i64 = ctypes.c_int64
+_f = ctypes.c_float
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        mf = [_f32p, _f32p, _f32p, _f32p, _f32p, _i64, _i64, _i64, _f, _f]
+        L.oracle_mf_forward_f64.argtypes = mf + [_f64p, _f64p]
+        L.oracle_mf_forward_f32.argtypes = mf + [_f32p, _f32p]
+        L.oracle_mf_backward_f64.argtypes = mf + [_f64p, _f64p]
+        L.oracle_mf_backward_f32.argtypes = mf + [_f32p, _f32p]
+        fft = [_f32p, _f32p, _f32p, _f32p, _f32p, _i64, _i64, _i64, _f, _f32p, _f32p]
+        L.oracle_mf_fft_forward_f32.argtypes = fft
+        L.oracle_mf_fft_backward_f32.argtypes = fft
+        tr = [_f32p, _f32p, _f32p, _f32p, _f32p, _u8p, _i64, _i64, _i64, _f, _f, _f]
+        L.oracle_tracer_forward_f64.argtypes = tr + [_f64p, _f64p]
+        L.oracle_tracer_forward_f32.argtypes = tr + [_f32p, _f32p]
+        trb = [_f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _u8p, _i64, _i64, _i64, _f, _f, _f]
+        L.oracle_tracer_backward_f64.argtypes = trb + [_f64p, _f64p, ctypes.c_void_p]
+        L.oracle_tracer_backward_f32.argtypes = trb + [_f32p, _f32p]
+        L.oracle_bilinear_forward_f32.argtypes = [_f32p, _f32p, _f32p, _f32p, _i64, _i64, _i64,
+                                                  _i64, _f32p, _f32p, _u8p]
+        L.oracle_bilinear_backward_f32.argtypes = [_f32p, _f32p, _f32p, _f32p, _i64, _i64, _i64,
+                                                   _i64, _f32p, _f32p]
+        L.oracle_num_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def num_threads() -> int:
+    return int(lib().oracle_num_threads())
+
+
+def _f32(x) -> np.ndarray:
+    return np.ascontiguousarray(x, dtype=np.float32)
+
+
+def _u8(x) -> np.ndarray:
+    return np.ascontiguousarray(x, dtype=np.uint8)
+
+
+# ---- matched filter ---------------------------------------------------------
+def mf_forward(real, imag, tx, rx, voxel_3n, fs, As, form="f64"):
+    """y[N] complex of the matched filter (MatchedFilter_cuda_kernel.cu:65-115)."""
+    real, imag, tx, rx, vox = map(_f32, (real, imag, tx, rx, voxel_3n))
+    A, S = real.shape
+    N = vox.shape[1]
+    dt = np.float64 if form == "f64" else np.float32
+    out_r = np.zeros(N, dt)
+    out_i = np.zeros(N, dt)
+    fn = lib().oracle_mf_forward_f64 if form == "f64" else lib().oracle_mf_forward_f32
+    fn(real, imag, tx, rx, vox, A, S, N, fs, As, out_r, out_i)
+    return out_r, out_i
+
+
+def mf_backward(grad_r, grad_i, tx, rx, voxel_3n, A, S, fs, As, form="f64"):
+    """grad[A,S] complex of the adjoint (MatchedFilter_cuda_kernel.cu:171-220)."""
+    gr, gi, tx, rx, vox = map(_f32, (grad_r, grad_i, tx, rx, voxel_3n))
+    N = vox.shape[1]
+    dt = np.float64 if form == "f64" else np.float32
+    out_r = np.zeros((A, S), dt)
+    out_i = np.zeros((A, S), dt)
+    fn = lib().oracle_mf_backward_f64 if form == "f64" else lib().oracle_mf_backward_f32
+    fn(gr, gi, tx, rx, vox, A, S, N, fs, As, out_r, out_i)
+    return out_r, out_i
+
+
+def mf_fft_forward(real, imag, tx, rx, voxel_3n, spacing):
+    real, imag, tx, rx, vox = map(_f32, (real, imag, tx, rx, voxel_3n))
+    A, B = real.shape
+    N = vox.shape[1]
+    out_r = np.zeros(N, np.float32)
+    out_i = np.zeros(N, np.float32)
+    lib().oracle_mf_fft_forward_f32(real, imag, tx, rx, vox, A, B, N, spacing, out_r, out_i)
+    return out_r, out_i
+
+
+def mf_fft_backward(grad_r, grad_i, tx, rx, voxel_3n, A, B, spacing):
+    gr, gi, tx, rx, vox = map(_f32, (grad_r, grad_i, tx, rx, voxel_3n))
+    N = vox.shape[1]
+    out_r = np.zeros((A, B), np.float32)
+    out_i = np.zeros((A, B), np.float32)
+    lib().oracle_mf_fft_backward_f32(gr, gi, tx, rx, vox, A, B, N, spacing, out_r, out_i)
+    return out_r, out_i
+
+
+# ---- signal tracer ----------------------------------------------------------
+def tracer_forward(normals, sigmas, points, tx, rx, inbounds, S, fs, f0, As, form="f64"):
+    """x[A,S] complex of the tracer (SignalTracer_cuda_kernel.cu:351-450)."""
+    normals, sigmas, points, tx, rx = map(_f32, (normals, sigmas, points, tx, rx))
+    inb = _u8(inbounds)
+    A, P = sigmas.shape
+    dt = np.float64 if form == "f64" else np.float32
+    out_r = np.zeros((A, S), dt)
+    out_i = np.zeros((A, S), dt)
+    fn = lib().oracle_tracer_forward_f64 if form == "f64" else lib().oracle_tracer_forward_f32
+    fn(normals, sigmas, points, tx, rx, inb, A, S, P, fs, f0, As, out_r, out_i)
+    return out_r, out_i
+
+
+def tracer_backward(grad_r, grad_i, normals, sigmas, points, tx, rx, inbounds, fs, f0, As,
+                    form="f64", with_points=True):
+    """(grad_normals [P,3], grad_sigmas [A,P], grad_points [P,3] or None)
+    (SignalTracer_cuda_kernel.cu:452-587; positions: no reference counterpart)."""
+    gr, gi, normals, sigmas, points, tx, rx = map(_f32, (grad_r, grad_i, normals, sigmas, points,
+                                                          tx, rx))
+    inb = _u8(inbounds)
+    A, P = sigmas.shape
+    S = gr.shape[1]
+    if form == "f64":
+        gn = np.zeros((P, 3), np.float64)
+        gs = np.zeros((A, P), np.float64)
+        gp = np.zeros((P, 3), np.float64) if with_points else None
+        lib().oracle_tracer_backward_f64(gr, gi, normals, sigmas, points, tx, rx, inb, A, S, P, fs,
+                                         f0, As, gn, gs,
+                                         gp.ctypes.data if gp is not None else None)
+        return gn, gs, gp
+    gn = np.zeros((P, 3), np.float32)
+    gs = np.zeros((A, P), np.float32)
+    lib().oracle_tracer_backward_f32(gr, gi, normals, sigmas, points, tx, rx, inb, A, S, P, fs, f0,
+                                     As, gn, gs)
+    return gn, gs, None
+
+
+# ---- along-ray resampler ---------------------------------------------------
+def bilinear_forward(normals, sigmas, z_vals, tgt_z_vals):
+    normals, sigmas, z, tz = map(_f32, (normals, sigmas, z_vals, tgt_z_vals))
+    R, S, _ = normals.shape
+    A = sigmas.shape[0]
+    T = tz.shape[1]
+    out_n = np.zeros((R, T, 3), np.float32)
+    out_s = np.zeros((A, R, T), np.float32)
+    out_b = np.zeros((R, T), np.uint8)
+    lib().oracle_bilinear_forward_f32(normals, sigmas, z, tz, A, R, S, T, out_n, out_s, out_b)
+    return out_n, out_s, out_b.astype(bool)
+
+
+def bilinear_backward(grad_out_normals, grad_out_sigmas, z_vals, tgt_z_vals, grad_normals=None,
+                      grad_sigmas=None):
+    gon, gos, z, tz = map(_f32, (grad_out_normals, grad_out_sigmas, z_vals, tgt_z_vals))
+    R, T, _ = gon.shape
+    A = gos.shape[0]
+    S = z.shape[1]
+    gn = _f32(grad_normals).copy() if grad_normals is not None else np.zeros((R, S, 3), np.float32)
+    gs = _f32(grad_sigmas).copy() if grad_sigmas is not None else np.zeros((A, R, S), np.float32)
+    lib().oracle_bilinear_backward_f32(gon, gos, z, tz, A, R, S, T, gn, gs)
+    return gn, gs
