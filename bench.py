@@ -52,6 +52,8 @@ def parse_args(argv=None):
     ap.add_argument("--workload", choices=["mf-full", "mf-small"], default="mf-full")
     ap.add_argument("--precision", choices=["mixed", "plain"], default="mixed")
     ap.add_argument("--no-extras", action="store_true", help="headline only (for profiling)")
+    ap.add_argument("--extras", default="plain,adjoint,tracer,cpu",
+                    help="comma list of secondary measurements: plain, adjoint, tracer, cpu")
     ap.add_argument("--seed", type=int, default=0)
     return ap.parse_args(argv)
 
@@ -333,9 +335,10 @@ def run_ours(args):
         "clocks": clock_info,
     }
 
-    if rank == 0 and not args.no_extras:
-        line.update(extras(args, wl, dev, out_r, out_i))
-        if world == 1:
+    wanted = set() if args.no_extras else {x.strip() for x in args.extras.split(",") if x.strip()}
+    if rank == 0 and wanted:
+        line.update(extras(args, wl, dev, out_r, out_i, wanted))
+        if world == 1 and "cpu" in wanted:
             line["cpu_baseline"], line["rel_err_vs_fp64"] = cpu_leg(wl, out_r, out_i, dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -345,18 +348,25 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def extras(args, wl, dev, out_r, out_i) -> dict:
+def extras(args, wl, dev, out_r, out_i, wanted) -> dict:
     """Secondary measurements: PLAIN form, MF adjoint, tracer fwd+adjoint."""
+    res = {}
+    if "plain" in wanted:
+        res.update(_plain_extra(wl, dev))
+    if "adjoint" in wanted:
+        res.update(_adjoint_extra(wl, dev))
+    if "tracer" in wanted:
+        res.update(_tracer_extra(args, dev))
+    return res
+
+
+def _plain_extra(wl, dev) -> dict:
     import torch
 
     from geraf_b200 import autotune
-    from geraf_b200.ops.RFMatchedFilter import _C as mfc
-    from geraf_b200.ops.RFSignalTracer import _C as trc
-    from geraf_b200.sdf import tracer_workload
 
     res = {}
     A, S, N = wl["A"], wl["S"], wl["N"]
-    ch = wl["chirp"]
     # PLAIN form on a voxel subset (it evaluates sinf/cosf per triple)
     n_sub = min(N, 16384)
     vsub = wl["voxel"][:, :n_sub].contiguous()
@@ -366,6 +376,18 @@ def extras(args, wl, dev, out_r, out_i) -> dict:
     ms = autotune.time_call(lambda: mf_call(wl, pr, pi, "plain", voxel=vsub, N=n_sub), iters=1, warmup=0)
     res["plain_form"] = {"value": round(float(A) * S * n_sub / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
                          "voxels": n_sub, "ms": round(ms, 2)}
+    return res
+
+
+def _adjoint_extra(wl, dev) -> dict:
+    import torch
+
+    from geraf_b200 import autotune
+    from geraf_b200.ops.RFMatchedFilter import _C as mfc
+
+    res = {}
+    A, S, N = wl["A"], wl["S"], wl["N"]
+    ch = wl["chirp"]
     # MF adjoint (mixed) on the full workload
     g_r = torch.randn(N, device=dev)
     g_i = torch.randn(N, device=dev)
@@ -380,6 +402,17 @@ def extras(args, wl, dev, out_r, out_i) -> dict:
     ms = autotune.time_call(adj, iters=1, warmup=1)
     res["mf_adjoint"] = {"value": round(float(A) * S * N / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
                          "ms": round(ms, 2), "precision": "mixed"}
+    return res
+
+
+def _tracer_extra(args, dev) -> dict:
+    import torch
+
+    from geraf_b200 import autotune
+    from geraf_b200.ops.RFSignalTracer import _C as trc
+    from geraf_b200.sdf import tracer_workload
+
+    res = {}
     # tracer forward + adjoint: 64 antennas x 4096 rays x 128 samples, S = 128
     tw = tracer_workload(device=dev, seed=args.seed)
     At, P, St = tw["A"], tw["P"], tw["chirp"].num_samples

@@ -140,6 +140,16 @@ __device__ __forceinline__ void align_point_gradient(const SpecGeom& g, const fl
   }
 }
 
+// Per-sample phase rate of the reference, w_n = 2*kPi*f0 + (2*kPi*As) * t_n
+// (SignalTracer_cuda_kernel.cu:375-377, 440).  The reference's compiled code
+// fuses the 2*kPi*f0 product into the sum and rounds the slope term first;
+// that rounding is pinned here with explicit intrinsics (it was identified
+// from the reference's outputs: it is the only choice that reproduces them).
+__device__ __forceinline__ float phase_rate(float f0, float As, float sample_time) {
+  const float phase_slope = 2.0f * kPiF * As;
+  return __fmaf_rn(2.0f * kPiF, f0, __fmul_rn(phase_slope, sample_time));
+}
+
 // ---------------------------------------------------------------------------
 template <typename T>
 struct TrP {
@@ -160,7 +170,6 @@ struct TrP {
   int* status;
   int64_t A, S, P;
   float fs, f0, As;
-  float phase_base, phase_slope;  // 2*kPi*f0 and 2*kPi*As in FP32, as the reference forms them
   double k0, b0, k1, b1;
   int splits;
   int64_t per_split;  // points (forward) or antennas (adjoint) per split
@@ -193,8 +202,7 @@ __global__ void __launch_bounds__(128) tracer_fwd_plain_kernel(const TrP<T> p) {
   load3(p.tx, a, txp);
   load3(p.rx, a, rxp);
   const float sample_time = static_cast<float>(n) / p.fs;
-  const float phase_base = p.phase_base;
-  const float phase_slope = p.phase_slope;
+  const float w = phase_rate(p.f0, p.As, sample_time);
   float acc_r = 0.0f, acc_i = 0.0f;
   for (int64_t p0 = 0; p0 < p.P; p0 += TILE) {
     const int count = static_cast<int>(min(static_cast<int64_t>(TILE), p.P - p0));
@@ -224,7 +232,7 @@ __global__ void __launch_bounds__(128) tracer_fwd_plain_kernel(const TrP<T> p) {
     if (active) {
       for (int i = 0; i < count; ++i) {
         if (!s_valid[i]) continue;
-        const float phase = (phase_base + phase_slope * sample_time) * s_tau[i];
+        const float phase = __fmul_rn(w, s_tau[i]);
         acc_r += s_amp[i] * cosf(phase);
         acc_i += s_amp[i] * sinf(phase);
       }
@@ -468,8 +476,6 @@ __global__ void __launch_bounds__(128) tracer_bwd_plain_kernel(const TrP<T> p) {
     load3(p.normals, pi, nrm);
     load3(p.points, pi, pt);
   }
-  const float phase_base = p.phase_base;
-  const float phase_slope = p.phase_slope;
   float accum_grad_normal[3] = {0.0f, 0.0f, 0.0f};
   float accum_grad_point[3] = {0.0f, 0.0f, 0.0f};
 
@@ -520,8 +526,8 @@ __global__ void __launch_bounds__(128) tracer_bwd_plain_kernel(const TrP<T> p) {
       float accum_tau = 0.0f;
       for (int n = 0; n < S; ++n) {
         const float sample_time = static_cast<float>(n) / p.fs;
-        const float omega = phase_base + phase_slope * sample_time;
-        const float phase = omega * tau;
+        const float omega = phase_rate(p.f0, p.As, sample_time);
+        const float phase = __fmul_rn(omega, tau);
         const float phase_real = cosf(phase);
         const float phase_imag = sinf(phase);
         const float gro = static_cast<float>(rowr[n]);
@@ -877,10 +883,6 @@ TrP<T> make_params(const TracerArgs& a) {
   p.fs = a.fs;
   p.f0 = a.f0;
   p.As = a.As;
-  // The reference forms these per thread as 2.0f * kPi * start_frequency and
-  // 2.0f * kPi * chirp_slope_scaled (FP32).
-  p.phase_base = 2.0f * kPiF * a.f0;
-  p.phase_slope = 2.0f * kPiF * a.As;
   const PhaseConsts pc = phase_consts(a.f0, a.As, a.fs);
   p.k0 = pc.k0;
   p.b0 = pc.b0;

@@ -32,3 +32,24 @@ def rel_l2(a, b):
     b = np.asarray(b, dtype=np.complex128) if np.iscomplexobj(b) else np.asarray(b, np.float64)
     den = np.linalg.norm(b.ravel())
     return float(np.linalg.norm((a - b).ravel()) / (den if den > 0 else 1.0))
+
+
+_PARITY = []
+
+
+@pytest.fixture
+def parity_log():
+    """Records measured parity figures; written to $GERAF_PARITY_OUT at session end."""
+    def log(test, **figures):
+        _PARITY.append({"test": test, **{k: (float(v) if not isinstance(v, str) else v)
+                                         for k, v in figures.items()}})
+    return log
+
+
+def pytest_sessionfinish(session, exitstatus):
+    path = os.environ.get("GERAF_PARITY_OUT")
+    if path and _PARITY:
+        import json
+
+        with open(path, "w") as f:
+            json.dump(_PARITY, f, indent=1)

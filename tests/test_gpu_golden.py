@@ -18,33 +18,48 @@ pytestmark = pytest.mark.gpu
 PLAIN_TOL = 1e-5
 
 
+def bitexact(a, b):
+    """Fraction of elements equal to the last bit (complex pairs count once)."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.mean(a == b))
+
+
 def _dtype(name):
     return {"f32": torch.float32, "f16": torch.float16, "f64": torch.float64}[name.rsplit("_", 1)[1]]
 
 
 @pytest.mark.parametrize("name", [c for c in golden_cases("mf_") if "fft" not in c])
-def test_mf_plain_matches_reference(cuda, name):
+def test_mf_plain_matches_reference(cuda, name, parity_log):
     g = load_golden(name)
     dt = _dtype(name)
     yr, yi = mf_forward(g["real"], g["imag"], g["tx"], g["rx"], g["voxel"], g["fs"], g["As"],
                         "plain", dt)
     ref = g["out_real"] + 1j * g["out_imag"]
     tol = PLAIN_TOL if dt != torch.float16 else 2e-3  # f16 outputs are rounded to 11 bits
-    assert rel_l2(yr + 1j * yi, ref) < tol
     A, S = g["real"].shape
     hr, hi = mf_backward(g["grad_output_real"], g["grad_output_imag"], g["tx"], g["rx"], g["voxel"],
                          A, S, g["fs"], g["As"], "plain", dt)
-    assert rel_l2(hr + 1j * hi, g["grad_real"] + 1j * g["grad_imag"]) < tol
+    e_f = rel_l2(yr + 1j * yi, ref)
+    e_b = rel_l2(hr + 1j * hi, g["grad_real"] + 1j * g["grad_imag"])
+    parity_log(f"mf_plain_vs_reference[{name}]", forward_rel_l2=e_f, adjoint_rel_l2=e_b,
+               forward_bitexact=bitexact(np.r_[yr, yi], np.r_[g["out_real"], g["out_imag"]]),
+               adjoint_bitexact=bitexact(np.r_[hr.ravel(), hi.ravel()],
+                                         np.r_[g["grad_real"].ravel(), g["grad_imag"].ravel()]))
+    assert e_f < tol
+    assert e_b < tol
 
 
 @pytest.mark.parametrize("name", [c for c in golden_cases("mf_") if "fft" not in c])
-def test_mf_mixed_close_to_reference(cuda, name):
+def test_mf_mixed_close_to_reference(cuda, name, parity_log):
     """The mixed form differs from the reference by about the reference's own FP32 error."""
     g = load_golden(name)
     dt = _dtype(name)
     yr, yi = mf_forward(g["real"], g["imag"], g["tx"], g["rx"], g["voxel"], g["fs"], g["As"],
                         "mixed", dt)
-    assert rel_l2(yr + 1j * yi, g["out_real"] + 1j * g["out_imag"]) < 1e-3
+    e = rel_l2(yr + 1j * yi, g["out_real"] + 1j * g["out_imag"])
+    parity_log(f"mf_mixed_vs_reference[{name}]", forward_rel_l2=e)
+    assert e < 1e-3
 
 
 @pytest.mark.parametrize("name", golden_cases("mf_fft"))
@@ -69,15 +84,23 @@ def test_mf_fft_matches_reference(cuda, name):
 
 
 @pytest.mark.parametrize("name", golden_cases("tracer_"))
-def test_tracer_plain_matches_reference(cuda, name):
+def test_tracer_plain_matches_reference(cuda, name, parity_log):
     g = load_golden(name)
     dt = _dtype(name)
     S = int(g["S"])
     xr, xi = tracer_forward(g, S, "plain", dt)
-    assert rel_l2(xr + 1j * xi, g["out_real"] + 1j * g["out_imag"]) < PLAIN_TOL
     gn, gs, _ = tracer_backward(g, g["grad_output_real"], g["grad_output_imag"], "plain", dt,
                                 with_points=False)
     inb = g["inbounds"].astype(bool)
+    parity_log(f"tracer_plain_vs_reference[{name}]",
+               forward_rel_l2=rel_l2(xr + 1j * xi, g["out_real"] + 1j * g["out_imag"]),
+               forward_bitexact=bitexact(np.r_[xr.ravel(), xi.ravel()],
+                                         np.r_[g["out_real"].ravel(), g["out_imag"].ravel()]),
+               grad_normals_rel_l2=rel_l2(gn[inb], g["grad_normals"][inb]),
+               grad_sigmas_rel_l2=rel_l2(gs[:, inb], g["grad_sigmas"][:, inb]),
+               grad_bitexact=bitexact(np.r_[gn[inb].ravel(), gs[:, inb].ravel()],
+                                      np.r_[g["grad_normals"][inb].ravel(), g["grad_sigmas"][:, inb].ravel()]))
+    assert rel_l2(xr + 1j * xi, g["out_real"] + 1j * g["out_imag"]) < PLAIN_TOL
     # the reference leaves out-of-bounds entries unwritten (NaN-prefilled); this library writes 0
     assert np.all(np.isnan(g["grad_normals"][~inb])) and np.all(gn[~inb] == 0)
     assert np.all(gs[:, ~inb] == 0)

@@ -140,13 +140,16 @@ def test_odd_sample_counts(cuda, S):
 
 
 def test_float64_and_float16_inputs(cuda, case):
+    """Other element types: the oracle sees the inputs rounded to that type
+    (half-precision voxel coordinates alone move the phase by ~0.5 rad)."""
     c, ch = case, case["ch"]
-    ref = orc.mf_forward(c["re"], c["im"], c["tx"], c["rx"], c["vox"], ch.adc_sample_rate, ch.As_sci)
-    ref = ref[0] + 1j * ref[1]
-    for dt, tol in ((torch.float64, MIXED_TOL), (torch.float16, 5e-3)):
+    for dt, npdt, tol in ((torch.float64, np.float64, MIXED_TOL), (torch.float16, np.float16, 2e-3)):
+        r = {k: c[k].astype(npdt).astype(np.float32) for k in ("re", "im", "tx", "rx", "vox")}
+        ref = orc.mf_forward(r["re"], r["im"], r["tx"], r["rx"], r["vox"], ch.adc_sample_rate, ch.As_sci)
         yr, yi = mf_forward(c["re"], c["im"], c["tx"], c["rx"], c["vox"], ch.adc_sample_rate, ch.As_sci,
                             "mixed", dtype=dt)
-        assert rel_l2(yr + 1j * yi, ref) < tol, dt
+        # half outputs carry 11-bit rounding (~3e-4 relative L2)
+        assert rel_l2(yr + 1j * yi, ref[0] + 1j * ref[1]) < tol, dt
 
 
 def test_empty_and_degenerate_sizes(cuda):

@@ -1,0 +1,123 @@
+"""Host-side logic that needs no GPU: arithmetic-form selection, the autotune
+cache, synthetic scenes, the SDF input generator's initialisation and the
+error behaviour of the drop-in wrappers on CPU tensors."""
+import json
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from geraf_b200 import autotune, runtime, scenes
+
+
+def test_precision_selection(monkeypatch):
+    monkeypatch.delenv("GERAF_RF_PRECISION", raising=False)
+    assert runtime.default_precision() == "mixed"
+    monkeypatch.setenv("GERAF_RF_PRECISION", "plain")
+    assert runtime.default_precision() == "plain"
+    with runtime.precision("mixed"):
+        assert runtime.default_precision() == "mixed"
+        assert runtime.mode_code(None) == 1
+    assert runtime.mode_code(None) == 0
+    with pytest.raises(ValueError):
+        with runtime.precision("fast"):
+            pass
+    monkeypatch.setenv("GERAF_RF_PRECISION", "bogus")
+    assert runtime.default_precision() == "mixed"
+
+
+def test_dtype_codes_and_errors():
+    assert runtime.dtype_code(torch.zeros(1), "op", True) == 0
+    assert runtime.dtype_code(torch.zeros(1, dtype=torch.float64), "op", True) == 1
+    assert runtime.dtype_code(torch.zeros(1, dtype=torch.float16), "op", True) == 2
+    with pytest.raises(RuntimeError, match="not implemented for 'Half'"):
+        runtime.dtype_code(torch.zeros(1, dtype=torch.float16), "op", False)
+    with pytest.raises(RuntimeError, match="not implemented"):
+        runtime.dtype_code(torch.zeros(1, dtype=torch.int32), "op", True)
+
+
+def test_autotune_cache_roundtrip(tmp_path, monkeypatch):
+    path = tmp_path / "tune.json"
+    monkeypatch.setenv("GERAF_RF_TUNE_CACHE", str(path))
+    autotune.clear()
+    assert autotune.lookup("mf_forward", (8, 4, 100), 1) is None
+    autotune.record("mf_forward", (8, 4, 100), 1, {"threads": 256, "items_per_thread": 2})
+    assert autotune.lookup("mf_forward", (8, 4, 100), 1)["threads"] == 256
+    data = json.loads(path.read_text())
+    assert any(k.startswith("mf_forward|1|8x4x100|") for k in data)
+    autotune.clear()
+    monkeypatch.setenv("GERAF_RF_TUNE_CACHE", str(path))
+    autotune._loaded_from = None
+    assert autotune.lookup("mf_forward", (8, 4, 100), 1)["items_per_thread"] == 2
+    # candidate lists are well-formed launch shapes
+    for c in autotune.mf_forward_candidates(1) + autotune.sample_major_candidates() + autotune.tracer_backward_candidates():
+        assert c["threads"] in (64, 128, 256)
+
+
+def test_virtual_arrays_and_grids():
+    tx, rx = scenes.virtual_array(16)
+    assert tx.shape == (3072, 3) and rx.shape == (3072, 3) and tx.dtype == np.float32
+    tx, rx = scenes.virtual_array(64)
+    assert tx.shape[0] == 49152
+    v = scenes.voxel_grid(48)
+    assert v.shape == (3, 48 ** 3)
+    assert np.isclose(v[2].mean(), 0.4, atol=1e-6) and np.isclose(v[0].max() - v[0].min(), 0.2, atol=1e-6)
+    ch = scenes.chirp(128)
+    assert math.isclose(ch.slope, 1.5625e14) and math.isclose(ch.As_sci, 1.5625e6)
+    assert math.isclose(scenes.chirp(256).As_sci, 7.8125e5)
+
+
+def test_shell_torus_scene():
+    rng = np.random.default_rng(0)
+    pos, amp = scenes.shell_torus_scene(rng)
+    assert pos.shape == (30000, 3) and amp.shape == (30000,)
+    rel = pos - np.array([0, 0, 0.4])
+    shell = np.abs(rel[:20000]).max(axis=1)
+    assert np.all(shell <= 0.15 + 1e-6) and np.all(shell >= 0.147 - 1e-6)
+    torus = rel[20000:]
+    ring = np.hypot(np.hypot(torus[:, 0], torus[:, 1]) - 0.08, torus[:, 2])
+    assert np.allclose(ring, 0.03, atol=1e-6)
+
+
+def test_sdf_geometric_init_is_a_sphere():
+    from geraf_b200.sdf import SDFNetwork
+
+    torch.manual_seed(0)
+    net = SDFNetwork()
+    x = torch.randn(512, 3)
+    x = x / x.norm(dim=1, keepdim=True) * torch.rand(512, 1)
+    sdf, feat = net(x)
+    assert feat.shape == (512, 256)
+    # approximately |x| - 0.5 (the init is exact only in the infinite-width limit)
+    target = x.norm(dim=1) - 0.5
+    dev = (sdf[:, 0] - target).detach()
+    assert dev.abs().mean() < 0.15
+    assert torch.corrcoef(torch.stack([sdf[:, 0].detach(), target]))[0, 1] > 0.9
+
+
+def test_wrappers_reject_cpu_tensors_before_any_gpu_call():
+    from geraf_b200.ops.RFMatchedFilter import matched_filter_cuda
+    from geraf_b200.ops.RFSignalTracer import signal_tracer_cuda
+
+    with pytest.raises(AssertionError, match="CUDA"):
+        matched_filter_cuda(torch.zeros(2, 4), torch.zeros(2, 4), torch.zeros(2, 3), torch.zeros(2, 3),
+                            torch.zeros(5, 3), 2, 4, 5e6, 1.0, 5)
+    with pytest.raises(ValueError, match="CUDA"):
+        signal_tracer_cuda(torch.zeros(5, 3), torch.zeros(2, 5), torch.zeros(5, 3), torch.zeros(2, 3),
+                           torch.zeros(2, 3), torch.ones(5, dtype=torch.bool), 4, 5e6, 770.0, 1.0, 2, 5)
+
+
+def test_model_utils_reject_other_backends():
+    from geraf_b200 import model_utils
+
+    cfg = scenes.chirp(8).radar_cfg()
+    with pytest.raises(ValueError, match="Only 'cuda'"):
+        model_utils.base_matched_filter(None, None, torch.zeros(1, 3), None, torch.zeros(1, 3), cfg,
+                                        backend="cpu")
+    with pytest.raises(ValueError, match="Only 'cuda'"):
+        model_utils.lensless_ray_tracer(torch.zeros(2, 3), None, torch.zeros(2, 3), torch.zeros(1, 3),
+                                        None, cfg, backend="numpy")
+    with pytest.raises(ValueError, match="Unsupported backend"):
+        model_utils.bilinear_ray_sampler(torch.zeros(1, 2, 3), torch.zeros(1, 1, 2), None,
+                                         torch.zeros(1, 2), backend="torch")
