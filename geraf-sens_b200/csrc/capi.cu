@@ -164,6 +164,8 @@ TracerArgs tracer_args(int64_t A, int64_t S, int64_t P, float fs, float f0, floa
 
 }  // namespace
 
+void set_last_error(const char* msg) { t_last_error = msg; }
+
 DeviceInfo current_device_info() {
   const int dev = current_device();
   ensure_device(dev);

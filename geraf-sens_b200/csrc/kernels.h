@@ -31,6 +31,9 @@ DeviceInfo current_device_info();
 // (looked up once per device; null if the lookup failed).
 int* device_status_ptr();
 
+// Sets the calling thread's message returned by geraf_rf_last_error().
+void set_last_error(const char* msg);
+
 // ---- matched filter ------------------------------------------------------
 struct MfArgs {
   const void* real;

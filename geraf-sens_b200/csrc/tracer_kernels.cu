@@ -150,6 +150,21 @@ __device__ __forceinline__ float phase_rate(float f0, float As, float sample_tim
   return __fmaf_rn(2.0f * kPiF, f0, __fmul_rn(phase_slope, sample_time));
 }
 
+// The same rate as the reference's adjoint forms it (SignalTracer_cuda_kernel.cu:552-554):
+// there the FP32 instantiation fuses the slope product instead,
+// fma(2*kPi*As, t_n, 2*kPi*f0), while the FP64 instantiation rounds as the
+// forward does.  Both were identified from the reference's outputs.
+template <typename T>
+__device__ __forceinline__ float adjoint_phase_rate(float f0, float As, float sample_time) {
+  return phase_rate(f0, As, sample_time);
+}
+template <>
+__device__ __forceinline__ float adjoint_phase_rate<float>(float f0, float As, float sample_time) {
+  const float phase_base = 2.0f * kPiF * f0;
+  const float phase_slope = 2.0f * kPiF * As;
+  return __fmaf_rn(phase_slope, sample_time, phase_base);
+}
+
 // ---------------------------------------------------------------------------
 template <typename T>
 struct TrP {
@@ -526,7 +541,7 @@ __global__ void __launch_bounds__(128) tracer_bwd_plain_kernel(const TrP<T> p) {
       float accum_tau = 0.0f;
       for (int n = 0; n < S; ++n) {
         const float sample_time = static_cast<float>(n) / p.fs;
-        const float omega = phase_rate(p.f0, p.As, sample_time);
+        const float omega = adjoint_phase_rate<T>(p.f0, p.As, sample_time);
         const float phase = __fmul_rn(omega, tau);
         const float phase_real = cosf(phase);
         const float phase_imag = sinf(phase);
