@@ -71,6 +71,9 @@ SIGNATURES = {
         [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _f32, _f32, _i64, _i32, _i32, _tp, _vp,
          ctypes.c_size_t, _vp],
     ),
+    "geraf_mf_forward_noalloc": (
+        _i32, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _f32, _f32, _i64, _vp]
+    ),
     "geraf_mf_backward_workspace_bytes": (_i32, [_i64, _i64, _i64, _i32, _i32, _tp, _szp]),
     "geraf_mf_backward": (
         _i32,

@@ -143,6 +143,25 @@ int32_t geraf_mf_fft_backward(const void* grad_output_real, const void* grad_out
                               float fft_spacing, float adc_sample_rate, float chirp_slope_scaled,
                               int64_t num_voxels, int32_t dtype, void* stream);
 
+/* Matched-filter forward (MIXED form, FP32 arrays) that allocates nothing and
+ * takes no workspace.  No counterpart in the reference.  It serves callers that
+ * cannot allocate device memory: hosts that fix their device-memory budget at
+ * start-up and own every buffer (e.g. a radar acquisition pipeline that may not
+ * allocate once it runs) and so cannot provide the problem-sized workspace
+ * geraf_mf_forward asks for.  The partial sums live in a 16 MiB array compiled
+ * into this library, which every GPU that loads the library holds until the
+ * process exits; hence num_voxels <= 1048576 (larger sizes return
+ * GERAF_ERR_INVALID_ARGUMENT).  The first call on each device looks up that
+ * array's device address (make it before any stream capture).  All calls share
+ * the array: calls that may overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller.  Arguments as for
+ * geraf_mf_forward. */
+int32_t geraf_mf_forward_noalloc(const void* real, const void* imag, const void* tx_pos,
+                                 const void* rx_pos, void* output_real, void* output_imag,
+                                 const void* voxel, int64_t total_ant_size,
+                                 int64_t num_adc_samples, float adc_sample_rate,
+                                 float chirp_slope_scaled, int64_t num_voxels, void* stream);
+
 /* ---- RFSignalTracer ----------------------------------------------------- */
 /* x[a,n] = (1/P) sum_{p in-bounds, not culled} sigma[a,p] * rho / D^2 * exp(+j (2 pi f0 + 2 pi As t_n) tau),
  * rho = <normalize(rx_a - p), normalize(i - 2 (i.n) n)>, i = normalize(p - tx_a),
