@@ -52,8 +52,9 @@ def parse_args(argv=None):
     ap.add_argument("--workload", choices=["mf-full", "mf-small"], default="mf-full")
     ap.add_argument("--precision", choices=["mixed", "plain"], default="mixed")
     ap.add_argument("--no-extras", action="store_true", help="headline only (for profiling)")
-    ap.add_argument("--extras", default="plain,adjoint,tracer,cpu",
-                    help="comma list of secondary measurements: plain, adjoint, tracer, cpu")
+    ap.add_argument("--extras", default="plain,adjoint,tracer,ragged,stage1,cpu",
+                    help="comma list of secondary measurements: plain, adjoint, tracer, ragged, "
+                         "stage1, cpu")
     ap.add_argument("--seed", type=int, default=0)
     return ap.parse_args(argv)
 
@@ -357,7 +358,87 @@ def extras(args, wl, dev, out_r, out_i, wanted) -> dict:
         res.update(_adjoint_extra(wl, dev))
     if "tracer" in wanted:
         res.update(_tracer_extra(args, dev))
+    if "ragged" in wanted:
+        res.update(_ragged_extra(args, dev))
+    if "stage1" in wanted:
+        res.update(_stage1_extra(args, dev))
     return res
+
+
+def ragged_workload(dev, seed=0, num_antennas=256, S=256):
+    """256 antennas of the 64x64x12 array, each with U[512, 8192] rays x U[64, 192]
+    samples (its own points) on the cube-shell + torus scene region, S = 256."""
+    import numpy as np
+    import torch
+
+    from geraf_b200 import scenes
+
+    rng = np.random.default_rng(seed)
+    tx, rx = scenes.virtual_array(64)
+    pick = np.sort(rng.choice(tx.shape[0], num_antennas, replace=False))
+    rays = rng.integers(512, 8193, num_antennas)
+    spr = rng.integers(64, 193, num_antennas)
+    counts = rays * spr
+    P = int(counts.sum())
+    g = torch.Generator(device=dev).manual_seed(seed)
+    ant = torch.repeat_interleave(torch.arange(num_antennas, device=dev), torch.tensor(counts, device=dev))
+    txd = torch.tensor(tx[pick], device=dev)
+    rxd = torch.tensor(rx[pick], device=dev)
+    aim = torch.tensor([0.0, 0.0, 0.4], device=dev) + (torch.rand((P, 3), device=dev, generator=g) - 0.5) * 0.3
+    org = rxd[ant]
+    pts = org + (aim - org) * (0.85 + 0.3 * torch.rand((P, 1), device=dev, generator=g))
+    nrm = torch.randn((P, 3), device=dev, generator=g)
+    nrm = nrm - 1.5 * (pts - org) / (pts - org).norm(dim=1, keepdim=True)  # mostly facing the radar
+    nrm = nrm / nrm.norm(dim=1, keepdim=True)
+    sig = torch.rand(P, device=dev, generator=g)
+    offs = torch.tensor(np.concatenate([[0], np.cumsum(counts)]).astype(np.int64), device=dev)
+    return dict(normals=nrm.contiguous(), sigmas=sig, points=pts.contiguous(), point_offsets=offs, tx=txd,
+                rx=rxd, rays=int(rays.sum()), P=P, S=S)
+
+
+def _ragged_extra(args, dev) -> dict:
+    """Batched uneven tracer + matched filter step (forward and adjoint), graph-captured."""
+    import torch
+
+    from geraf_b200 import autotune, scenes
+    from geraf_b200.step import RaggedRFStep
+
+    w = ragged_workload(dev, args.seed)
+    ch = scenes.chirp(w["S"])
+    vox = torch.tensor(scenes.voxel_grid(64, size=0.32).T.copy(), device=dev)
+    step = RaggedRFStep(w["normals"], w["sigmas"], w["points"], w["point_offsets"], w["tx"], w["rx"], vox,
+                        torch.full((vox.shape[0],), 1e-4, device=dev), ch.radar_cfg(fc_start=770.0))
+    step.capture()
+    ms = autotune.time_call(step.run, iters=3, warmup=1)
+    A = w["tx"].shape[0]
+    return {"ragged_step": {
+        "workload": (f"{A} antennas, rays U[512,8192] x samples U[64,192] per antenna "
+                     f"({w['rays']} rays, {w['P']} points), S={w['S']}, MF onto 64^3 voxels"),
+        "ms": round(ms, 3), "rays_per_s": round(w["rays"] / (ms * 1e-3), 1),
+        "point_samples_per_s_G": round(float(w["P"]) * w["S"] / (ms * 1e-3) / 1e9, 2),
+        "graph": True}}
+
+
+def _stage1_extra(args, dev) -> dict:
+    """End-to-end stage-1 RF training step: mixed + CUDA graph vs plain eager."""
+    import torch
+
+    from geraf_b200 import autotune, scenes
+    from geraf_b200.step import Stage1RFStep
+
+    res = {}
+    vox = torch.tensor(scenes.voxel_grid(128, size=0.32).T.copy(), device=dev)
+    target = torch.ones(vox.shape[0], device=dev)
+    for name, prec, graph, iters in (("mixed_graph", "mixed", True, 5), ("plain_eager", "plain", False, 1)):
+        st = Stage1RFStep(num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=256, voxels=vox,
+                          target_mag=target, precision=prec, device=dev, seed=args.seed)
+        if graph:
+            st.capture()
+        ms = autotune.time_call(st.run, iters=iters, warmup=1)
+        res[name] = {"ms": round(ms, 2), "it_per_s": round(1e3 / ms, 2)}
+    return {"stage1_step": {"workload": ("128 antennas x 2048 rays x 128 samples, S=256, random-init "
+                                         "SDF MLP, MF onto 128^3 voxels, L1 on |volume|, Adam"),
+                            **res}}
 
 
 def _plain_extra(wl, dev) -> dict:

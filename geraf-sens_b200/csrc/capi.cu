@@ -495,6 +495,100 @@ GERAF_EXPORT int32_t geraf_tracer_backward(const void* grad_output_real, const v
                        "signal_tracer_backward launch");
 }
 
+// ---- batched tracer over uneven per-antenna point sets ----------------------------
+namespace {
+int32_t check_ragged(int64_t A, int64_t S, int64_t P, int32_t dtype) {
+  REQUIRE(A >= 0 && S >= 0 && P >= 0, "sizes must be non-negative");
+  REQUIRE(A <= kI32Max && P <= (int64_t{1} << 40), "sizes out of range");
+  REQUIRE(S <= 1024, "the batched tracer supports at most 1024 ADC samples");
+  REQUIRE(!(A == 0 && P > 0), "points given but no antennas: point_offsets cannot be valid");
+  if (!valid_dtype(dtype, false)) {
+    return fail(GERAF_ERR_INVALID_ARGUMENT,
+                std::string("\"signal_tracer_ragged\" not implemented for '") + dtype_name(dtype) + "'");
+  }
+  return GERAF_OK;
+}
+}  // namespace
+
+GERAF_EXPORT int32_t geraf_tracer_ragged_workspace_bytes(int64_t A, int64_t S, int64_t P,
+                                                         int32_t dtype, size_t* bytes) {
+  if (bytes == nullptr) return fail(GERAF_ERR_INVALID_ARGUMENT, "bytes is null");
+  if (int32_t rc = check_ragged(A, S, P, dtype)) return rc;
+  *bytes = tracer_ragged_workspace(A, S, P);
+  return GERAF_OK;
+}
+
+GERAF_EXPORT int32_t geraf_tracer_forward_ragged(
+    const void* normals, const void* sigmas, const void* points, const int64_t* point_offsets,
+    const void* tx_pos, const void* rx_pos, const uint8_t* inbounds, void* output_real,
+    void* output_imag, int64_t num_adc_samples, float adc_sample_rate, float start_frequency,
+    float chirp_slope_scaled, int64_t total_ant_size, int64_t total_point_size, int32_t dtype,
+    void* workspace, size_t workspace_bytes, void* stream) {
+  if (int32_t rc = check_ragged(total_ant_size, num_adc_samples, total_point_size, dtype)) return rc;
+  if (total_ant_size > 0 && num_adc_samples > 0) {
+    REQUIRE(output_real && output_imag && tx_pos && rx_pos && point_offsets,
+            "output, antenna and offset pointers must be non-null");
+    if (total_point_size > 0) REQUIRE(normals && sigmas && points, "point pointers must be non-null");
+  }
+  RaggedArgs a{};
+  a.normals = normals;
+  a.sigmas = sigmas;
+  a.points = points;
+  a.offsets = point_offsets;
+  a.tx = tx_pos;
+  a.rx = rx_pos;
+  a.inbounds = inbounds;
+  a.out_real = output_real;
+  a.out_imag = output_imag;
+  a.A = total_ant_size;
+  a.S = num_adc_samples;
+  a.P = total_point_size;
+  a.fs = adc_sample_rate;
+  a.f0 = start_frequency;
+  a.As = chirp_slope_scaled;
+  a.dtype = dtype;
+  if (int32_t rc = check_workspace(tracer_ragged_workspace(a.A, a.S, a.P), workspace, workspace_bytes)) return rc;
+  return finish_launch(tracer_forward_ragged(a, workspace, static_cast<cudaStream_t>(stream)),
+                       "signal_tracer_forward_ragged launch");
+}
+
+GERAF_EXPORT int32_t geraf_tracer_backward_ragged(
+    const void* grad_output_real, const void* grad_output_imag, const void* normals,
+    const void* sigmas, const void* points, const int64_t* point_offsets, const void* tx_pos,
+    const void* rx_pos, const uint8_t* inbounds, void* grad_normals, void* grad_sigmas,
+    void* grad_points, int64_t num_adc_samples, float adc_sample_rate, float start_frequency,
+    float chirp_slope_scaled, int64_t total_ant_size, int64_t total_point_size, int32_t dtype,
+    void* stream) {
+  if (int32_t rc = check_ragged(total_ant_size, num_adc_samples, total_point_size, dtype)) return rc;
+  if (total_point_size > 0) {
+    REQUIRE(grad_normals && grad_sigmas && normals && sigmas && points && point_offsets && tx_pos &&
+                rx_pos && (num_adc_samples == 0 || (grad_output_real && grad_output_imag)),
+            "pointers must be non-null");
+  }
+  RaggedArgs a{};
+  a.grad_real_out = grad_output_real;
+  a.grad_imag_out = grad_output_imag;
+  a.normals = normals;
+  a.sigmas = sigmas;
+  a.points = points;
+  a.offsets = point_offsets;
+  a.tx = tx_pos;
+  a.rx = rx_pos;
+  a.inbounds = inbounds;
+  a.grad_normals = grad_normals;
+  a.grad_sigmas = grad_sigmas;
+  a.grad_points = grad_points;
+  a.A = total_ant_size;
+  a.S = num_adc_samples;
+  a.P = total_point_size;
+  a.fs = adc_sample_rate;
+  a.f0 = start_frequency;
+  a.As = chirp_slope_scaled;
+  a.dtype = dtype;
+  return finish_launch(tracer_backward_ragged(a, static_cast<cudaStream_t>(stream)),
+                       "signal_tracer_backward_ragged launch");
+}
+
 GERAF_EXPORT int32_t geraf_bilinear_forward(const void* normals, const void* sigmas,
                                             const void* z_vals, const void* target_z_vals,
                                             void* output_normals, void* output_sigmas,

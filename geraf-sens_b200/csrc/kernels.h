@@ -103,6 +103,30 @@ Tuning tracer_backward_resolve(const TracerArgs& a, const Tuning& req);
 size_t tracer_backward_workspace(const TracerArgs& a, const Tuning& t);
 cudaError_t tracer_backward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st);
 
+// Batched tracer over antennas with uneven point sets (CSR point_offsets [A+1]).
+struct RaggedArgs {
+  const void* normals;      // [P,3]
+  const void* sigmas;       // [P]
+  const void* points;       // [P,3]
+  const int64_t* offsets;   // [A+1]
+  const void* tx;           // [A,3]
+  const void* rx;
+  const uint8_t* inbounds;  // [P] or null
+  void* out_real;           // forward: [A,S]
+  void* out_imag;
+  const void* grad_real_out;  // backward: [A,S]
+  const void* grad_imag_out;
+  void* grad_normals;  // backward: [P,3]
+  void* grad_sigmas;   // backward: [P]
+  void* grad_points;   // backward: [P,3] or null
+  int64_t A, S, P;
+  float fs, f0, As;
+  int dtype;
+};
+size_t tracer_ragged_workspace(int64_t A, int64_t S, int64_t P);
+cudaError_t tracer_forward_ragged(const RaggedArgs& a, void* ws, cudaStream_t st);
+cudaError_t tracer_backward_ragged(const RaggedArgs& a, cudaStream_t st);
+
 struct BilinearArgs {
   const void* normals;  // fwd: [R,S,3] in; bwd: grad_output_normals [R,T,3]
   const void* sigmas;   // fwd: [A,R,S] in; bwd: grad_output_sigmas [A,R,T]

@@ -821,7 +821,10 @@ cudaError_t launch_fft(const MfFftArgs& a, bool backward, cudaStream_t st) {
 Tuning mf_forward_resolve(const MfArgs& a, const Tuning& req) {
   Tuning t = req;
   if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 128;
-  if (t.items != 1 && t.items != 2 && t.items != 4) t.items = a.mode == kMixed ? 2 : 1;
+  // Four voxels per thread amortise the shared-memory sample loads and loop
+  // control of the Horner loop over more FMAs (measured best on B200 for both
+  // the 3072 x 128 and the 49152 x 256 workloads).
+  if (t.items != 1 && t.items != 2 && t.items != 4) t.items = a.mode == kMixed ? 4 : 1;
   if (t.stage_rows <= 0) t.stage_rows = 8;
   t.stage_rows = std::min(t.stage_rows, 64);
   const int64_t rows_total = std::max<int64_t>(1, (a.A + t.stage_rows - 1) / t.stage_rows);

@@ -203,6 +203,44 @@ int32_t geraf_tracer_backward(const void* grad_output_real, const void* grad_out
                               int32_t mode, const geraf_tuning_t* tuning, void* workspace,
                               size_t workspace_bytes, void* stream);
 
+/* Batched tracer over all antennas of a step, each with its own uneven set of
+ * points (MIXED form).  Points of antenna 0 come first, then antenna 1, ...;
+ * point_offsets [A+1] (int64, CSR, offsets[0] = 0, offsets[A] = P,
+ * non-decreasing) delimits them.  normals, points: [P,3]; sigmas: [P] (each
+ * point's amplitude weight for its own antenna); inbounds: [P] or NULL (all
+ * in bounds); output [A,S]; S <= 1024.  Row a equals geraf_tracer_forward
+ * over antenna a's points alone (normalised by that antenna's point count;
+ * an antenna without points gives NaN, as 0/0 in the reference).  One
+ * persistent launch load-balances the uneven antennas; malformed offsets are
+ * detected on the device (no point is read; device status word = 1).
+ * Replaces a loop of SignalTracer::SignalTracer_forward calls, one per antenna
+ * (SignalTracer_cuda.cu:314-356): the batched entry point has no single
+ * counterpart in the reference. */
+int32_t geraf_tracer_ragged_workspace_bytes(int64_t total_ant_size, int64_t num_adc_samples,
+                                            int64_t total_point_size, int32_t dtype,
+                                            size_t* bytes);
+int32_t geraf_tracer_forward_ragged(const void* normals, const void* sigmas, const void* points,
+                                    const int64_t* point_offsets, const void* tx_pos,
+                                    const void* rx_pos, const uint8_t* inbounds, void* output_real,
+                                    void* output_imag, int64_t num_adc_samples,
+                                    float adc_sample_rate, float start_frequency,
+                                    float chirp_slope_scaled, int64_t total_ant_size,
+                                    int64_t total_point_size, int32_t dtype, void* workspace,
+                                    size_t workspace_bytes, void* stream);
+/* Adjoint of geraf_tracer_forward_ragged: grad_sigmas [P], grad_normals [P,3]
+ * and, when non-NULL, grad_points [P,3]; out-of-bounds points get zeros.
+ * Replaces the per-antenna SignalTracer::SignalTracer_backward_normal_sigma
+ * calls (SignalTracer_cuda.cu:358-406). */
+int32_t geraf_tracer_backward_ragged(const void* grad_output_real, const void* grad_output_imag,
+                                     const void* normals, const void* sigmas, const void* points,
+                                     const int64_t* point_offsets, const void* tx_pos,
+                                     const void* rx_pos, const uint8_t* inbounds,
+                                     void* grad_normals, void* grad_sigmas, void* grad_points,
+                                     int64_t num_adc_samples, float adc_sample_rate,
+                                     float start_frequency, float chirp_slope_scaled,
+                                     int64_t total_ant_size, int64_t total_point_size,
+                                     int32_t dtype, void* stream);
+
 /* Linear resampling along rays: for each ray and target depth, bracket the
  * target in the ray's coarse depths by binary search and interpolate sigma
  * (all A rows) and normals; out-of-range targets give 0 and inbounds = 0.
