@@ -28,11 +28,14 @@ namespace {
 // ---------------------------------------------------------------------------
 // Shared-memory layout of the voxel-major forward kernels.
 struct FwdSmem {
-  size_t pos_off, kn_off, buf_off, total;
+  size_t pos_off, kn_off, buf_off, dup_off, total;
 };
 
+// MIXED (`dup`): after the TMA ring, one [2][rows][ld] float2 buffer holding
+// every staged sample twice, (s, s), so that one 16-byte shared load yields
+// the broadcast operands of two packed FMAs.
 template <typename T, typename PosT>
-FwdSmem fwd_smem_layout(int rows, int ld, bool with_kn) {
+FwdSmem fwd_smem_layout(int rows, int ld, bool with_kn, bool dup) {
   FwdSmem s;
   s.pos_off = 128;  // two mbarriers, padded
   size_t off = s.pos_off + 2 * static_cast<size_t>(rows) * 6 * sizeof(PosT);
@@ -42,6 +45,9 @@ FwdSmem fwd_smem_layout(int rows, int ld, bool with_kn) {
   off = (off + 127) & ~static_cast<size_t>(127);
   s.buf_off = off;
   off += 4 * static_cast<size_t>(rows) * ld * sizeof(T);
+  off = (off + 127) & ~static_cast<size_t>(127);
+  s.dup_off = off;
+  if (dup) off += 2 * static_cast<size_t>(rows) * ld * sizeof(float2);
   s.total = (off + 127) & ~static_cast<size_t>(127);
   return s;
 }
@@ -62,7 +68,7 @@ struct MfFwdP {
   double k0, b0, k1, b1;
   int rows, ld, splits, bulk;
   int64_t ant_per_split;
-  size_t pos_off, kn_off, buf_off;
+  size_t pos_off, kn_off, buf_off, dup_off;
 };
 
 __device__ __forceinline__ float sq(float x) { return x * x; }
@@ -80,13 +86,21 @@ __device__ __forceinline__ void stage_positions(PosT* pos, int stage, int rows_m
 }
 
 // ---------------------------------------------------------------------------
-// MIXED forward: VPT voxels per thread, antennas streamed through a
-// double-buffered TMA ring of `rows` antennas x S samples.
+// MIXED forward: VPT voxels per thread (VPT even), antennas streamed through a
+// double-buffered TMA ring of `rows` antennas x S samples.  After each stage
+// lands, the block expands it into the duplicated (s, s) layout; the Horner
+// loop then runs on voxel PAIRS with packed FMAs:
+//   P <- P z + s,  per pair (a, b):  t1 = PI (-ZI) + SR;  t2 = PI ZR + SI;
+//                                     PR' = PR ZR + t1;  PI' = PR ZI + t2
+// which is exactly the scalar recurrence, two voxels per instruction.
 template <typename T, int VPT>
 __global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
+  static_assert(VPT % 2 == 0, "voxels are processed in packed pairs");
+  constexpr int PAIRS = VPT / 2;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
   double* pos = reinterpret_cast<double*>(smem + p.pos_off);
+  float2* dup = reinterpret_cast<float2*>(smem + p.dup_off);  // [2][rows][ld]
   PairStager<T> stg{reinterpret_cast<T*>(smem + p.buf_off), bar, p.ld, p.rows, p.bulk != 0};
 
   const int split = blockIdx.x % p.splits;
@@ -94,6 +108,7 @@ __global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
   const int64_t a_begin = static_cast<int64_t>(split) * p.ant_per_split;
   const int64_t a_end = min(p.A, a_begin + p.ant_per_split);
   const int ntiles = a_end > a_begin ? ceil_div(a_end - a_begin, p.rows) : 0;
+  const int S = static_cast<int>(p.S);
 
   if (p.bulk && threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
@@ -102,15 +117,15 @@ __global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
   }
   __syncthreads();
 
-  double vx[VPT], vy[VPT], vz[VPT];
+  float vx[VPT], vy[VPT], vz[VPT];
   int64_t vid[VPT];
 #pragma unroll
   for (int j = 0; j < VPT; ++j) {
     vid[j] = vtile * blockDim.x * VPT + threadIdx.x + static_cast<int64_t>(j) * blockDim.x;
     const bool ok = vid[j] < p.N;
-    vx[j] = ok ? static_cast<double>(ld_f(p.voxel, vid[j])) : 0.0;
-    vy[j] = ok ? static_cast<double>(ld_f(p.voxel, p.N + vid[j])) : 0.0;
-    vz[j] = ok ? static_cast<double>(ld_f(p.voxel, 2 * p.N + vid[j])) : 0.0;
+    vx[j] = ok ? ld_f(p.voxel, vid[j]) : 0.0f;
+    vy[j] = ok ? ld_f(p.voxel, p.N + vid[j]) : 0.0f;
+    vz[j] = ok ? ld_f(p.voxel, 2 * p.N + vid[j]) : 0.0f;
   }
   float yr[VPT], yi[VPT], cr[VPT], ci[VPT];
 #pragma unroll
@@ -119,12 +134,13 @@ __global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
   auto issue = [&](int tile, int stage) {
     const int64_t a0 = a_begin + static_cast<int64_t>(tile) * p.rows;
     const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
-    stg.issue(stage, p.real, p.imag, a0, rws, static_cast<int>(p.S));
+    stg.issue(stage, p.real, p.imag, a0, rws, S);
     stage_positions<T, double>(pos, stage, p.rows, p.tx, p.rx, a0, rws);
   };
   if (ntiles > 0) issue(0, 0);
   if (ntiles > 1) issue(1, 1);
 
+  const int rows_ld = p.rows * p.ld;
   for (int t = 0; t < ntiles; ++t) {
     const int s = t & 1;
     if (!stg.wait(s, (t >> 1) & 1, p.status)) {
@@ -133,57 +149,82 @@ __global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
     }
     const int64_t a0 = a_begin + static_cast<int64_t>(t) * p.rows;
     const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
-    const T* sre = stg.stage_ptr(s, 0);
-    const T* sim = stg.stage_ptr(s, 1);
-    for (int r = 0; r < rws; ++r) {
-      const double* ps = pos + (s * p.rows + r) * 6;
-      const double tx = ps[0], ty = ps[1], tz = ps[2], rx = ps[3], ry = ps[4], rz = ps[5];
-      float2 e0[VPT], z[VPT];
-      float pr[VPT], pi[VPT];
-#pragma unroll
-      for (int j = 0; j < VPT; ++j) {
-        const PhaseCycles pc = path_cycles(tx - vx[j], ty - vy[j], tz - vz[j], rx - vx[j],
-                                           ry - vy[j], rz - vz[j], p.k0, p.b0, p.k1, p.b1);
-        const float2 c0 = cis_cycles(pc.frac0);
-        const float2 c1 = cis_cycles(pc.dcyc);
-        e0[j] = make_float2(c0.x, -c0.y);  // exp(-j phi0)
-        z[j] = make_float2(c1.x, -c1.y);   // exp(-j dphi)
-        pr[j] = 0.0f;
-        pi[j] = 0.0f;
-      }
-      const T* rowr = sre + r * p.ld;
-      const T* rowi = sim + r * p.ld;
-      // Horner from the highest sample down: P <- P z + s[n].  Padded
-      // samples (n >= S) are zero and leave P at zero.
-#pragma unroll 2
-      for (int n = p.ld - 4; n >= 0; n -= 4) {
-        const float4 a = lds4(rowr + n);
-        const float4 b = lds4(rowi + n);
-#pragma unroll
-        for (int j = 0; j < VPT; ++j) {
-          float nr, ni;
-          nr = fmaf(pr[j], z[j].x, fmaf(-pi[j], z[j].y, a.w));
-          ni = fmaf(pr[j], z[j].y, fmaf(pi[j], z[j].x, b.w));
-          pr[j] = nr; pi[j] = ni;
-          nr = fmaf(pr[j], z[j].x, fmaf(-pi[j], z[j].y, a.z));
-          ni = fmaf(pr[j], z[j].y, fmaf(pi[j], z[j].x, b.z));
-          pr[j] = nr; pi[j] = ni;
-          nr = fmaf(pr[j], z[j].x, fmaf(-pi[j], z[j].y, a.y));
-          ni = fmaf(pr[j], z[j].y, fmaf(pi[j], z[j].x, b.y));
-          pr[j] = nr; pi[j] = ni;
-          nr = fmaf(pr[j], z[j].x, fmaf(-pi[j], z[j].y, a.x));
-          ni = fmaf(pr[j], z[j].y, fmaf(pi[j], z[j].x, b.x));
-          pr[j] = nr; pi[j] = ni;
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < VPT; ++j) {
-        const float2 term = cmul(e0[j], make_float2(pr[j], pi[j]));
-        kahan_add(yr[j], cr[j], term.x);
-        kahan_add(yi[j], ci[j], term.y);
+    {  // expand the stage into (s, s) pairs; samples past S stay zero
+      const T* sre = stg.stage_ptr(s, 0);
+      const T* sim = stg.stage_ptr(s, 1);
+      for (int i = threadIdx.x; i < rws * p.ld; i += blockDim.x) {
+        const int c = i % p.ld;
+        const float vr = c < S ? static_cast<float>(sre[i]) : 0.0f;
+        const float vi = c < S ? static_cast<float>(sim[i]) : 0.0f;
+        dup[i] = make_float2(vr, vr);
+        dup[rows_ld + i] = make_float2(vi, vi);
       }
     }
     __syncthreads();
+    for (int r = 0; r < rws; ++r) {
+      const double* ps = pos + (s * p.rows + r) * 6;
+      const double tx = ps[0], ty = ps[1], tz = ps[2], rx = ps[3], ry = ps[4], rz = ps[5];
+      float frac0[VPT];
+      float2 ZR[PAIRS], ZI[PAIRS], NZI[PAIRS], PR[PAIRS], PI[PAIRS];
+#pragma unroll
+      for (int q = 0; q < PAIRS; ++q) {
+        float zr2[2], zi2[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = 2 * q + h;
+          const double dx = static_cast<double>(vx[j]), dy = static_cast<double>(vy[j]),
+                       dz = static_cast<double>(vz[j]);
+          const PhaseCycles pc =
+              path_cycles(tx - dx, ty - dy, tz - dz, rx - dx, ry - dy, rz - dz, p.k0, p.b0, p.k1, p.b1);
+          const float2 c1 = cis_cycles(pc.dcyc);
+          frac0[j] = pc.frac0;
+          zr2[h] = c1.x;
+          zi2[h] = -c1.y;  // z = exp(-j dphi)
+        }
+        ZR[q] = make_float2(zr2[0], zr2[1]);
+        ZI[q] = make_float2(zi2[0], zi2[1]);
+        NZI[q] = make_float2(-zi2[0], -zi2[1]);
+        PR[q] = make_float2(0.0f, 0.0f);
+        PI[q] = make_float2(0.0f, 0.0f);
+      }
+      const float2* rowr = dup + r * p.ld;
+      const float2* rowi = dup + rows_ld + r * p.ld;
+      // Horner from the highest sample down; padded samples are zero.
+#pragma unroll 2
+      for (int n = p.ld - 2; n >= 0; n -= 2) {
+        const float4 a = *reinterpret_cast<const float4*>(rowr + n);  // (s_n, s_n, s_n+1, s_n+1)
+        const float4 b = *reinterpret_cast<const float4*>(rowi + n);
+        const float2 sr1 = make_float2(a.z, a.w), si1 = make_float2(b.z, b.w);
+        const float2 sr0 = make_float2(a.x, a.y), si0 = make_float2(b.x, b.y);
+#pragma unroll
+        for (int q = 0; q < PAIRS; ++q) {
+          float2 t1 = ffma2(PI[q], NZI[q], sr1);
+          float2 t2 = ffma2(PI[q], ZR[q], si1);
+          float2 npr = ffma2(PR[q], ZR[q], t1);
+          PI[q] = ffma2(PR[q], ZI[q], t2);
+          PR[q] = npr;
+          t1 = ffma2(PI[q], NZI[q], sr0);
+          t2 = ffma2(PI[q], ZR[q], si0);
+          npr = ffma2(PR[q], ZR[q], t1);
+          PI[q] = ffma2(PR[q], ZI[q], t2);
+          PR[q] = npr;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < PAIRS; ++q) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = 2 * q + h;
+          const float2 c0 = cis_cycles(frac0[j]);
+          const float2 e0 = make_float2(c0.x, -c0.y);  // exp(-j phi0)
+          const float2 pv = h == 0 ? make_float2(PR[q].x, PI[q].x) : make_float2(PR[q].y, PI[q].y);
+          const float2 term = cmul(e0, pv);
+          kahan_add(yr[j], cr[j], term.x);
+          kahan_add(yi[j], ci[j], term.y);
+        }
+      }
+    }
+    __syncthreads();  // stage s (raw samples and positions) and dup are free again
     if (t + 2 < ntiles) issue(t + 2, s);
   }
 
@@ -615,9 +656,9 @@ struct FwdShape {
 template <typename T>
 const void* fwd_kernel_ptr(int mode, int vpt) {
   if (mode == kMixed) {
-    if (vpt == 1) return reinterpret_cast<const void*>(&mf_fwd_mixed_kernel<T, 1>);
-    if (vpt == 2) return reinterpret_cast<const void*>(&mf_fwd_mixed_kernel<T, 2>);
-    return reinterpret_cast<const void*>(&mf_fwd_mixed_kernel<T, 4>);
+    if (vpt <= 2) return reinterpret_cast<const void*>(&mf_fwd_mixed_kernel<T, 2>);
+    if (vpt == 4) return reinterpret_cast<const void*>(&mf_fwd_mixed_kernel<T, 4>);
+    return reinterpret_cast<const void*>(&mf_fwd_mixed_kernel<T, 8>);
   }
   if (vpt == 1) return reinterpret_cast<const void*>(&mf_fwd_plain_kernel<T, 1>);
   if (vpt == 2) return reinterpret_cast<const void*>(&mf_fwd_plain_kernel<T, 2>);
@@ -637,12 +678,12 @@ FwdShape fwd_shape(const MfArgs& a, const Tuning& t) {
   s.rows = t.stage_rows;
   const bool mixed = a.mode == kMixed;
   auto layout = [&](int rows) {
-    if (a.dtype == kF64) return mixed ? fwd_smem_layout<double, double>(rows, s.ld, false)
-                                      : fwd_smem_layout<double, float>(rows, s.ld, true);
-    if (a.dtype == kF16) return mixed ? fwd_smem_layout<__half, double>(rows, s.ld, false)
-                                      : fwd_smem_layout<__half, float>(rows, s.ld, true);
-    return mixed ? fwd_smem_layout<float, double>(rows, s.ld, false)
-                 : fwd_smem_layout<float, float>(rows, s.ld, true);
+    if (a.dtype == kF64) return mixed ? fwd_smem_layout<double, double>(rows, s.ld, false, true)
+                                      : fwd_smem_layout<double, float>(rows, s.ld, true, false);
+    if (a.dtype == kF16) return mixed ? fwd_smem_layout<__half, double>(rows, s.ld, false, true)
+                                      : fwd_smem_layout<__half, float>(rows, s.ld, true, false);
+    return mixed ? fwd_smem_layout<float, double>(rows, s.ld, false, true)
+                 : fwd_smem_layout<float, float>(rows, s.ld, true, false);
   };
   const DeviceInfo dev = current_device_info();
   s.layout = layout(s.rows);
@@ -687,6 +728,7 @@ cudaError_t launch_fwd(const MfArgs& a, const FwdShape& s, void* ws, cudaStream_
   p.pos_off = s.layout.pos_off;
   p.kn_off = s.layout.kn_off;
   p.buf_off = s.layout.buf_off;
+  p.dup_off = s.layout.dup_off;
 
   const void* fn = fwd_kernel_ptr<T>(a.mode, s.vpt);
   cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -821,10 +863,16 @@ cudaError_t launch_fft(const MfFftArgs& a, bool backward, cudaStream_t st) {
 Tuning mf_forward_resolve(const MfArgs& a, const Tuning& req) {
   Tuning t = req;
   if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 128;
-  // Four voxels per thread amortise the shared-memory sample loads and loop
-  // control of the Horner loop over more FMAs (measured best on B200 for both
-  // the 3072 x 128 and the 49152 x 256 workloads).
-  if (t.items != 1 && t.items != 2 && t.items != 4) t.items = a.mode == kMixed ? 4 : 1;
+  // MIXED runs voxel pairs through packed FMAs (2, 4 or 8 voxels per thread);
+  // eight amortise the shared-memory sample loads, loop control and the
+  // per-(voxel, antenna) phase set-up best (measured on B200: 128 threads x 8
+  // voxels x 8-antenna stages is the fastest shape for 49152 x 256 samples
+  // x 128^3 voxels).  PLAIN takes 1, 2 or 4.
+  if (a.mode == kMixed) {
+    if (t.items != 2 && t.items != 4 && t.items != 8) t.items = t.items == 1 ? 2 : 8;
+  } else if (t.items != 1 && t.items != 2 && t.items != 4) {
+    t.items = 1;
+  }
   if (t.stage_rows <= 0) t.stage_rows = 8;
   t.stage_rows = std::min(t.stage_rows, 64);
   const int64_t rows_total = std::max<int64_t>(1, (a.A + t.stage_rows - 1) / t.stage_rows);

@@ -105,8 +105,8 @@ def tune(op: str, sizes: tuple, mode: int, run: Callable[[dict], None],
 
 def mf_forward_candidates(mode: int) -> list[dict]:
     out = []
-    for threads in (128, 256):
-        for items in ((1, 2, 4) if mode == 1 else (1, 2)):
+    for threads in (64, 128, 256):
+        for items in ((2, 4, 8) if mode == 1 else (1, 2)):
             for rows in (4, 8, 16):
                 out.append({"threads": threads, "items_per_thread": items, "stage_rows": rows})
     return out

@@ -1,9 +1,7 @@
 """RFMatchedFilter: FMCW matched-filter backprojection (sm_100a).
 
-Lazy exports, as in the reference (``geraf/ops/RFMatchedFilter/__init__.py:6-18``).
+Exports as in the reference (``geraf/ops/RFMatchedFilter/__init__.py:6-18``).
 """
-from importlib import import_module
-
 _EXPORTS = {
     "matched_filter_cuda": ".matched_filter_cuda",
     "faster_matched_filter_cuda": ".faster_matched_filter_cuda",
@@ -12,11 +10,10 @@ _EXPORTS = {
 __all__ = list(_EXPORTS)
 
 
-def __getattr__(name):
-    if name not in _EXPORTS:
-        raise AttributeError(name)
-    fn = getattr(import_module(_EXPORTS[name], __name__), name)
-    # Importing the submodule binds its module object under the same name;
-    # rebind the function so later `from ... import name` keeps returning it.
-    globals()[name] = fn
-    return fn
+# The exported functions share their submodules' names.  Importing them here,
+# once, binds the package attribute to the function after the import system has
+# bound it to the submodule; later imports of the submodule leave it alone.  The
+# compiled library is still loaded lazily, at the first operator call.
+from .matched_filter_cuda import matched_filter_cuda  # noqa: E402
+from .faster_matched_filter_cuda import faster_matched_filter_cuda  # noqa: E402
+

@@ -1,9 +1,7 @@
 """RFSignalTracer: lensless specular RF renderer and along-ray resampler (sm_100a).
 
-Lazy exports, as in the reference (``geraf/ops/RFSignalTracer/__init__.py:6-18``).
+Exports as in the reference (``geraf/ops/RFSignalTracer/__init__.py:6-18``).
 """
-from importlib import import_module
-
 _EXPORTS = {
     "signal_tracer_cuda": ".signal_tracer_cuda",
     "bilinear_raysample_cuda": ".bilinear_raysample_cuda",
@@ -12,11 +10,10 @@ _EXPORTS = {
 __all__ = list(_EXPORTS)
 
 
-def __getattr__(name):
-    if name not in _EXPORTS:
-        raise AttributeError(name)
-    fn = getattr(import_module(_EXPORTS[name], __name__), name)
-    # Importing the submodule binds its module object under the same name;
-    # rebind the function so later `from ... import name` keeps returning it.
-    globals()[name] = fn
-    return fn
+# The exported functions share their submodules' names.  Importing them here,
+# once, binds the package attribute to the function after the import system has
+# bound it to the submodule; later imports of the submodule leave it alone.  The
+# compiled library is still loaded lazily, at the first operator call.
+from .signal_tracer_cuda import signal_tracer_cuda  # noqa: E402
+from .bilinear_raysample_cuda import bilinear_raysample_cuda  # noqa: E402
+

@@ -162,7 +162,10 @@ class Stage1RFStep(_Graphable):
         cdf = torch.sigmoid(sdf * inv_s)
         alpha = ((cdf[:, :-1] - cdf[:, 1:]) / (cdf[:, :-1] + 1e-5)).clamp(0.0, 1.0)
         alpha = torch.cat([alpha, alpha[:, -1:]], 1)
-        trans = torch.cumprod(torch.cat([torch.ones_like(alpha[:, :1]), 1.0 - alpha + 1e-7], 1), 1)[:, :-1]
+        # transmittance prod_{j<i} (1 - alpha_j); formed as exp(cumsum(log)) because the
+        # backward of cumprod synchronises with the host, which stream capture forbids
+        log_t = torch.log(1.0 - alpha + 1e-7)
+        trans = torch.exp(torch.cumsum(log_t, 1) - log_t)
         sig = (alpha * trans * torch.sigmoid(self.head(feat)).reshape(self.R, self.T)).reshape(1, -1)
         P = self.R * self.T
         xr, xi = signal_tracer_cuda(normals, sig.expand(A, P).contiguous(), self.points, self.tx, self.rx,

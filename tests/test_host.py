@@ -121,3 +121,34 @@ def test_model_utils_reject_other_backends():
     with pytest.raises(ValueError, match="Unsupported backend"):
         model_utils.bilinear_ray_sampler(torch.zeros(1, 2, 3), torch.zeros(1, 1, 2), None,
                                          torch.zeros(1, 2), backend="torch")
+
+
+def test_volume_grid_layout_matches_reference_reshape():
+    """Flat index = (ix * Ny + iy) * Nz + iz, as np.fromfile(...).reshape(nx, ny, nz) reads it."""
+    from geraf_b200 import volume
+
+    bound = [0.5, 0.503, -0.37, -0.368, -0.15, -0.146]
+    res = [0.001, 0.001, 0.002]
+    assert volume.grid_shape(bound, res) == (4, 3, 3)
+    v = volume.grid_voxels(bound, res).numpy()
+    nx, ny, nz = volume.grid_shape(bound, res)
+    g = v.reshape(nx, ny, nz, 3)
+    assert np.allclose(g[2, 1, 0], [0.502, -0.369, -0.15], atol=1e-7)
+    assert np.allclose(g[3, 2, 2], [0.503, -0.368, -0.146], atol=1e-7)
+    part = volume.grid_voxels(bound, res, start=5, count=7).numpy()
+    assert np.array_equal(part, v[5:12])
+    with pytest.raises(ValueError):
+        volume.grid_num(1.0, 0.0, 0.0)
+
+
+def test_sarimage_roundtrip_and_sampling(tmp_path):
+    from geraf_b200 import volume
+
+    vol = torch.arange(4 * 3 * 5, dtype=torch.float32).reshape(4, 3, 5)
+    p = tmp_path / "sarimage.bin"
+    volume.write_sarimage(str(p), vol)
+    assert np.array_equal(volume.read_sarimage(str(p), (4, 3, 5)), vol.numpy())
+    # corners of the normalised cube hit the corner voxels (align_corners=True)
+    pts = torch.tensor([[-1.0, -1.0, -1.0], [1.0, 1.0, 1.0], [1.0, -1.0, 1.0]])
+    got = volume.sample_volume(vol, pts)
+    assert torch.allclose(got, torch.tensor([vol[0, 0, 0], vol[3, 2, 4], vol[3, 0, 4]]))
