@@ -52,9 +52,9 @@ def parse_args(argv=None):
     ap.add_argument("--workload", choices=["mf-full", "mf-small"], default="mf-full")
     ap.add_argument("--precision", choices=["mixed", "plain"], default="mixed")
     ap.add_argument("--no-extras", action="store_true", help="headline only (for profiling)")
-    ap.add_argument("--extras", default="plain,adjoint,tracer,ragged,stage1,cpu",
-                    help="comma list of secondary measurements: plain, adjoint, tracer, ragged, "
-                         "stage1, cpu")
+    ap.add_argument("--extras", default="plain,adjoint,nufft,tracer,ragged,stage1,cpu",
+                    help="comma list of secondary measurements: plain, adjoint, nufft, tracer, "
+                         "ragged, stage1, cpu")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     return ap.parse_args(argv)
@@ -381,6 +381,8 @@ def extras(args, wl, dev, out_r, out_i, wanted) -> dict:
         res.update(_plain_extra(wl, dev))
     if "adjoint" in wanted:
         res.update(_adjoint_extra(wl, dev))
+    if "nufft" in wanted:
+        res.update(_nufft_extra(wl, dev, out_r, out_i))
     if "tracer" in wanted:
         res.update(_tracer_extra(args, dev))
     if "ragged" in wanted:
@@ -508,6 +510,46 @@ def _adjoint_extra(wl, dev) -> dict:
     ms = autotune.time_call(adj, iters=1, warmup=1)
     res["mf_adjoint"] = {"value": round(float(A) * S * N / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
                          "ms": round(ms, 2), "precision": "mixed"}
+    return res
+
+
+def _nufft_extra(wl, dev, out_r, out_i) -> dict:
+    """The matched filter's fast approximate form (oversampled range FFT + 8-point
+    ES interpolation) on the full workload: forward and adjoint times, in the
+    headline's unit (the same voxel x antenna x sample sums, evaluated in O(W)
+    per voxel-antenna pair), and their relative L2 against the MIXED form over
+    every output element (the MIXED form is itself ~2e-7 from FP64)."""
+    import torch
+
+    from geraf_b200 import autotune
+    from geraf_b200.ops.RFMatchedFilter import _C as mfc
+
+    A, S, N = wl["A"], wl["S"], wl["N"]
+    ch = wl["chirp"]
+    yr = torch.empty(N, device=dev)
+    yi = torch.empty(N, device=dev)
+    ms = autotune.time_call(lambda: mf_call(wl, yr, yi, "nufft"), iters=2, warmup=1)
+    ref = torch.complex(out_r.double(), out_i.double())
+    err = float((torch.complex(yr.double(), yi.double()) - ref).norm() / ref.norm())
+    res = {"mf_forward_nufft": {"value": round(float(A) * S * N / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                                "ms": round(ms, 2), "taps": 8, "rel_l2_vs_mixed": err}}
+    g_r = torch.randn(N, device=dev)
+    g_i = torch.randn(N, device=dev)
+    h_r = torch.empty((A, S), device=dev)
+    h_i = torch.empty((A, S), device=dev)
+    m_r = torch.empty((A, S), device=dev)
+    m_i = torch.empty((A, S), device=dev)
+
+    def adj(prec, hr, hi):
+        mfc.MatchedFilter_backward_realimag(g_r, g_i, wl["real"], wl["imag"], wl["tx"], wl["rx"], hr, hi,
+                                            wl["voxel"], A, S, ch.adc_sample_rate, ch.As_sci, N, precision=prec)
+
+    ms_b = autotune.time_call(lambda: adj("nufft", h_r, h_i), iters=2, warmup=1)
+    adj("mixed", m_r, m_i)
+    ref_b = torch.complex(m_r.double(), m_i.double())
+    err_b = float((torch.complex(h_r.double(), h_i.double()) - ref_b).norm() / ref_b.norm())
+    res["mf_adjoint_nufft"] = {"value": round(float(A) * S * N / (ms_b * 1e-3) / 1e9, 3), "unit": UNIT,
+                               "ms": round(ms_b, 2), "taps": 8, "rel_l2_vs_mixed": err_b}
     return res
 
 

@@ -74,6 +74,7 @@ Tuning to_tuning(const geraf_tuning_t* t) {
     out.stage_rows = t->stage_rows;
     out.splits = t->splits;
     out.chunk = t->chunk;
+    out.taps = t->taps;
   }
   return out;
 }
@@ -115,7 +116,11 @@ int32_t check_mf_sizes(int64_t A, int64_t S, int64_t N, int32_t dtype, int32_t m
     return fail(GERAF_ERR_INVALID_ARGUMENT,
                 std::string("\"matched_filter\" not implemented for '") + dtype_name(dtype) + "'");
   }
-  REQUIRE(mode == GERAF_MODE_PLAIN || mode == GERAF_MODE_MIXED, "mode must be PLAIN or MIXED");
+  REQUIRE(mode == GERAF_MODE_PLAIN || mode == GERAF_MODE_MIXED || mode == GERAF_MODE_NUFFT,
+          "mode must be PLAIN, MIXED or NUFFT");
+  if (mode == GERAF_MODE_NUFFT && !mf_nufft_supported(S)) {
+    return fail(GERAF_ERR_UNSUPPORTED, "NUFFT matched filter needs num_adc_samples <= 4096");
+  }
   return GERAF_OK;
 }
 

@@ -250,6 +250,19 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
 
+// Stages the tx and rx positions of `rws` antennas from a0 into slot `stage`
+// of a [2][rows_max][6] shared table, as PosT (float or double).
+template <typename T, typename PosT>
+__device__ __forceinline__ void stage_positions(PosT* pos, int stage, int rows_max, const T* tx,
+                                                const T* rx, int64_t a0, int rws) {
+  for (int i = threadIdx.x; i < rws * 6; i += blockDim.x) {
+    const int r = i / 6;
+    const int c = i - r * 6;
+    const T* src = c < 3 ? tx : rx;
+    pos[(stage * rows_max + r) * 6 + c] = static_cast<PosT>(ld_f(src, (a0 + r) * 3 + (c % 3)));
+  }
+}
+
 // Kahan-compensated accumulation of one component.
 __device__ __forceinline__ void kahan_add(float& sum, float& comp, float x) {
   const float y = x - comp;

@@ -11,7 +11,7 @@
 namespace geraf {
 
 enum DType : int { kF32 = 0, kF64 = 1, kF16 = 2 };
-enum Mode : int { kPlain = 0, kMixed = 1 };
+enum Mode : int { kPlain = 0, kMixed = 1, kNufft = 2 };
 
 struct Tuning {
   int threads = 0;
@@ -19,6 +19,7 @@ struct Tuning {
   int stage_rows = 0;  // antenna rows per shared-memory stage
   int splits = 0;      // partial-sum splits of the reduced dimension
   int chunk = 0;       // samples per lane (sample-major kernels)
+  int taps = 0;        // interpolation kernel width (NUFFT matched filter)
 };
 
 struct DeviceInfo {
@@ -53,6 +54,22 @@ struct MfArgs {
 Tuning mf_forward_resolve(const MfArgs& a, const Tuning& req);
 size_t mf_forward_workspace(const MfArgs& a, const Tuning& t);
 cudaError_t mf_forward(const MfArgs& a, const Tuning& t, void* ws, cudaStream_t st);
+
+// Fast approximate matched filter (MODE_NUFFT, nufft_kernels.cu); the generic
+// mf_forward_* entry points dispatch here for that mode.
+constexpr int64_t kNufftMaxSamples = 4096;
+bool mf_nufft_supported(int64_t S);
+Tuning mf_nufft_forward_resolve(const MfArgs& a, const Tuning& req);
+size_t mf_nufft_forward_workspace(const MfArgs& a, const Tuning& t);
+cudaError_t mf_nufft_forward(const MfArgs& a, const Tuning& t, void* ws, cudaStream_t st);
+Tuning mf_nufft_backward_resolve(const MfArgs& a, const Tuning& req);
+size_t mf_nufft_backward_workspace(const MfArgs& a, const Tuning& t);
+cudaError_t mf_nufft_backward(const MfArgs& a, const Tuning& t, void* ws, cudaStream_t st);
+
+// Sums `splits` float2 partials per element in split order (FP64), divides by
+// `divisor` and stores in the element type.
+cudaError_t launch_finalize_partials(int dtype, const float2* partial, int splits, int64_t count,
+                                     float divisor, void* out_r, void* out_i, cudaStream_t st);
 
 Tuning mf_backward_resolve(const MfArgs& a, const Tuning& req);
 size_t mf_backward_workspace(const MfArgs& a, const Tuning& t);

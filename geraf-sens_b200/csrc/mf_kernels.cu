@@ -73,18 +73,6 @@ struct MfFwdP {
 
 __device__ __forceinline__ float sq(float x) { return x * x; }
 
-// Stages antenna positions of one tile as PosT (float for PLAIN, double for MIXED).
-template <typename T, typename PosT>
-__device__ __forceinline__ void stage_positions(PosT* pos, int stage, int rows_max, const T* tx,
-                                                const T* rx, int64_t a0, int rws) {
-  for (int i = threadIdx.x; i < rws * 6; i += blockDim.x) {
-    const int r = i / 6;
-    const int c = i - r * 6;
-    const T* src = c < 3 ? tx : rx;
-    pos[(stage * rows_max + r) * 6 + c] = static_cast<PosT>(ld_f(src, (a0 + r) * 3 + (c % 3)));
-  }
-}
-
 // ---------------------------------------------------------------------------
 // MIXED forward: VPT voxels per thread (VPT even), antennas streamed through a
 // double-buffered TMA ring of `rows` antennas x S samples.  After each stage
@@ -860,7 +848,27 @@ cudaError_t launch_fft(const MfFftArgs& a, bool backward, cudaStream_t st) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+cudaError_t launch_finalize_partials(int dtype, const float2* partial, int splits, int64_t count,
+                                     float divisor, void* out_r, void* out_i, cudaStream_t st) {
+  const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((count + 255) / 256, 148 * 16)));
+  switch (dtype) {
+    case kF64:
+      finalize_partials_kernel<double><<<blocks, 256, 0, st>>>(
+          partial, splits, count, divisor, static_cast<double*>(out_r), static_cast<double*>(out_i));
+      break;
+    case kF16:
+      finalize_partials_kernel<__half><<<blocks, 256, 0, st>>>(
+          partial, splits, count, divisor, static_cast<__half*>(out_r), static_cast<__half*>(out_i));
+      break;
+    default:
+      finalize_partials_kernel<float><<<blocks, 256, 0, st>>>(
+          partial, splits, count, divisor, static_cast<float*>(out_r), static_cast<float*>(out_i));
+  }
+  return cudaGetLastError();
+}
+
 Tuning mf_forward_resolve(const MfArgs& a, const Tuning& req) {
+  if (a.mode == kNufft) return mf_nufft_forward_resolve(a, req);
   Tuning t = req;
   if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 128;
   // MIXED runs voxel pairs through packed FMAs (2, 4 or 8 voxels per thread);
@@ -889,11 +897,13 @@ Tuning mf_forward_resolve(const MfArgs& a, const Tuning& req) {
 }
 
 size_t mf_forward_workspace(const MfArgs& a, const Tuning& t) {
+  if (a.mode == kNufft) return mf_nufft_forward_workspace(a, t);
   if (t.splits <= 1 || a.N == 0) return 0;
   return static_cast<size_t>(t.splits) * a.N * sizeof(float2);
 }
 
 cudaError_t mf_forward(const MfArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  if (a.mode == kNufft) return mf_nufft_forward(a, t, ws, st);
   if (a.N == 0) return cudaSuccess;
   const FwdShape s = fwd_shape(a, t);
   switch (a.dtype) {
@@ -904,6 +914,7 @@ cudaError_t mf_forward(const MfArgs& a, const Tuning& t, void* ws, cudaStream_t 
 }
 
 Tuning mf_backward_resolve(const MfArgs& a, const Tuning& req) {
+  if (a.mode == kNufft) return mf_nufft_backward_resolve(a, req);
   Tuning t = req;
   if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 256;
   if (t.chunk != 8 && t.chunk != 16 && t.chunk != 32) t.chunk = 16;
@@ -927,11 +938,13 @@ Tuning mf_backward_resolve(const MfArgs& a, const Tuning& req) {
 }
 
 size_t mf_backward_workspace(const MfArgs& a, const Tuning& t) {
+  if (a.mode == kNufft) return mf_nufft_backward_workspace(a, t);
   if (a.mode == kPlain || t.splits <= 1) return 0;
   return static_cast<size_t>(t.splits) * a.A * a.S * sizeof(float2);
 }
 
 cudaError_t mf_backward(const MfArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  if (a.mode == kNufft) return mf_nufft_backward(a, t, ws, st);
   if (a.A == 0 || a.S == 0) return cudaSuccess;
   switch (a.dtype) {
     case kF64: return launch_bwd<double>(a, t, ws, st);

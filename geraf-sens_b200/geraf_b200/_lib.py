@@ -26,6 +26,7 @@ DTYPE_F16 = 2
 
 MODE_PLAIN = 0
 MODE_MIXED = 1
+MODE_NUFFT = 2
 
 
 class Tuning(ctypes.Structure):
@@ -37,6 +38,7 @@ class Tuning(ctypes.Structure):
         ("stage_rows", ctypes.c_int32),
         ("splits", ctypes.c_int32),
         ("chunk", ctypes.c_int32),
+        ("taps", ctypes.c_int32),
     ]
 
     def as_dict(self) -> dict:

@@ -7,9 +7,10 @@ error behaviour (``RuntimeError`` with the reference's TORCH_CHECK messages) as
 ``csrc/matched_filter/MatchedFilter_cuda.cu:10-343``.  Each call runs on the
 current torch stream of the input's device and does not synchronise.
 
-Extra keyword-only arguments (not in the reference): ``precision`` ("mixed" or
-"plain", default from :func:`geraf_b200.runtime.default_precision`) and
-``tuning`` (a launch-shape dict, default from the autotuner cache).
+Extra keyword-only arguments (not in the reference): ``precision`` ("mixed",
+"plain" or "nufft", default from :func:`geraf_b200.runtime.default_precision`)
+and ``tuning`` (a launch-shape dict, default from the autotuner cache; for
+"nufft" its ``taps`` key sets the interpolation width, 4 to 12, default 8).
 """
 from __future__ import annotations
 
@@ -101,7 +102,7 @@ def MatchedFilter_forward(real, imag, tx_pos, rx_pos, output_real, output_imag, 
     A, S, N = int(total_ant_size), int(num_adc_samples), int(num_voxels)
     _check_forward(real, imag, tx_pos, rx_pos, output_real, output_imag, voxel, A, S, N)
     dt = dtype_code(real, "matched_filter_forward_cuda", allow_half=True)
-    mode = mode_code(precision)
+    mode = mode_code(precision, allow_nufft=True)
     tun = tuning_struct("mf_forward", (A, S, N), mode, tuning)
     with device_guard(real.device):
         nbytes = _lib.workspace_bytes("geraf_mf_forward_workspace_bytes", A, S, N, dt, mode,
@@ -122,7 +123,7 @@ def MatchedFilter_backward_realimag(grad_output_real, grad_output_imag, real, im
     _check_backward(grad_output_real, grad_output_imag, real, imag, tx_pos, rx_pos, grad_real,
                     grad_imag, voxel, A, S, N)
     dt = dtype_code(real, "matched_filter_backward_realimag_cuda", allow_half=True)
-    mode = mode_code(precision)
+    mode = mode_code(precision, allow_nufft=True)
     tun = tuning_struct("mf_backward", (A, S, N), mode, tuning)
     with device_guard(real.device):
         nbytes = _lib.workspace_bytes("geraf_mf_backward_workspace_bytes", A, S, N, dt, mode,

@@ -9,8 +9,11 @@ Semantics kept from the reference:
   * the backward pass produces gradients for ``real`` and ``image`` only, and
     only when both require grad (``matched_filter_cuda.py:175``); it is
     once-differentiable.
-Addition: keyword ``precision`` ("mixed" / "plain"; default from
-``geraf_b200.runtime.default_precision``) and ``tuning``.
+Addition: keyword ``precision`` ("mixed" / "plain" / "nufft"; default from
+``geraf_b200.runtime.default_precision``) and ``tuning``.  The form is fixed
+when the forward runs; the backward uses the same form and, for "nufft", the
+same interpolation width (``tuning["taps"]``), so it is the adjoint of the
+forward that ran.
 """
 from __future__ import annotations
 
@@ -20,6 +23,7 @@ import torch
 from torch.autograd import Function
 from torch.autograd.function import once_differentiable
 
+from ...runtime import default_precision
 from . import _C
 
 
@@ -60,7 +64,8 @@ class _MatchedFilterKernel(Function):
 
         ctx.save_for_backward(real, image, tpos, rpos, voxel_soa)
         ctx.sizes = (total_ant_size, numADCSample, adcSampleRate, As_sci, N)
-        ctx.precision = precision
+        ctx.precision = precision or default_precision()
+        ctx.taps = (tuning or {}).get("taps")
         return output_real, output_image
 
     @staticmethod
@@ -80,7 +85,7 @@ class _MatchedFilterKernel(Function):
             _C.MatchedFilter_backward_realimag(
                 grad_output_real, grad_output_image, real, image, tpos, rpos, grad_real,
                 grad_image, voxel_soa, total_ant_size, numADCSample, adcSampleRate, As_sci, N,
-                precision=ctx.precision)
+                precision=ctx.precision, tuning={"taps": ctx.taps} if ctx.taps else None)
         return (grad_real, grad_image) + (None,) * 10
 
 

@@ -1,6 +1,6 @@
 """Host-side plumbing shared by the operator modules: tensor checks with the
 reference's error wording, dtype / stream / workspace handling, the arithmetic
-form (PLAIN / MIXED) selection and tuned launch shapes.
+form (PLAIN / MIXED / NUFFT) selection and tuned launch shapes.
 
 PyTorch supplies device memory (its caching allocator, so workspaces are
 CUDA-graph safe), the current stream and autograd; every byte of compute runs
@@ -26,16 +26,20 @@ _DTYPE_NAMES = {torch.float32: "Float", torch.float64: "Double", torch.float16: 
 
 _state = threading.local()
 
-PRECISIONS = ("mixed", "plain")
+PRECISIONS = ("mixed", "plain", "nufft")
+_MODES = {"mixed": _lib.MODE_MIXED, "plain": _lib.MODE_PLAIN, "nufft": _lib.MODE_NUFFT}
 
 
 def default_precision() -> str:
     """Arithmetic form used when a call does not name one.
 
     ``mixed`` (FP64 phase reduction, Horner / rotator phasors, compensated
-    sums; judged against an FP64 oracle) unless ``GERAF_RF_PRECISION=plain``
-    (the reference's FP32 arithmetic, expression for expression) is set or a
-    :func:`precision` context is active.
+    sums; judged against an FP64 oracle) unless ``GERAF_RF_PRECISION`` names
+    ``plain`` (the reference's FP32 arithmetic, expression for expression) or
+    ``nufft`` (the matched filter's fast approximate form: MIXED phases, the
+    sample sum through an oversampled range FFT and a short interpolation
+    kernel; other operators run ``mixed`` under it), or a :func:`precision`
+    context is active.
     """
     override = getattr(_state, "precision", None)
     if override is not None:
@@ -57,11 +61,18 @@ def precision(mode: str):
         _state.precision = prev
 
 
-def mode_code(precision_: str | None) -> int:
+def mode_code(precision_: str | None, allow_nufft: bool = False) -> int:
+    """C-ABI arithmetic form of a call.  ``nufft`` exists for the matched
+    filter only: named explicitly elsewhere it is an error, as the ambient
+    default it means ``mixed``."""
     p = precision_ or default_precision()
     if p not in PRECISIONS:
         raise ValueError(f"precision must be one of {PRECISIONS}, got {p!r}")
-    return _lib.MODE_MIXED if p == "mixed" else _lib.MODE_PLAIN
+    if p == "nufft" and not allow_nufft:
+        if precision_ is not None:
+            raise ValueError("precision 'nufft' is only available for the matched filter")
+        p = "mixed"
+    return _MODES[p]
 
 
 def dtype_code(t: torch.Tensor, op: str, allow_half: bool) -> int:

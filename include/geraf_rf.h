@@ -59,6 +59,15 @@ extern "C" {
  *        (relative L2 <= 1e-4).                                              */
 #define GERAF_MODE_PLAIN 0
 #define GERAF_MODE_MIXED 1
+/* NUFFT (matched filter only; no reference counterpart): the MIXED phase
+ *        model with the per-antenna sample sum evaluated through an
+ *        oversampled range FFT of each antenna's samples and a W-point
+ *        "exponential of semicircle" interpolation kernel, O(W) instead of
+ *        O(S) work per (voxel, antenna).  A fast approximate form: relative
+ *        L2 against the FP64 oracle ~1e-6 at W = 8 (tuning.taps), ~1e-3 at
+ *        W = 4.  Needs num_adc_samples <= 4096.  The adjoint is the exact
+ *        adjoint of this forward.                                          */
+#define GERAF_MODE_NUFFT 2
 
 /* Launch shape.  Any field left 0 takes the library default for the call. */
 typedef struct geraf_tuning {
@@ -67,6 +76,7 @@ typedef struct geraf_tuning {
   int32_t stage_rows;       /* antenna rows per shared-memory stage                     */
   int32_t splits;           /* partial-sum splits of the reduced dimension              */
   int32_t chunk;            /* samples per lane in the sample-major kernels: 8,16,32    */
+  int32_t taps;             /* NUFFT interpolation width W: 4, 6, 8, 10 or 12           */
 } geraf_tuning_t;
 
 /* ---- library information ---------------------------------------------- */

@@ -27,6 +27,16 @@ def test_precision_selection(monkeypatch):
     assert runtime.default_precision() == "mixed"
 
 
+def test_nufft_form_is_matched_filter_only(monkeypatch):
+    monkeypatch.setenv("GERAF_RF_PRECISION", "nufft")
+    assert runtime.default_precision() == "nufft"
+    assert runtime.mode_code(None, allow_nufft=True) == 2
+    assert runtime.mode_code(None) == 1  # ambient nufft: the tracer runs mixed
+    with pytest.raises(ValueError, match="matched filter"):
+        runtime.mode_code("nufft")
+    assert runtime.mode_code("nufft", allow_nufft=True) == 2
+
+
 def test_dtype_codes_and_errors():
     assert runtime.dtype_code(torch.zeros(1), "op", True) == 0
     assert runtime.dtype_code(torch.zeros(1, dtype=torch.float64), "op", True) == 1
