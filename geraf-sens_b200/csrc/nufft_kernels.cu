@@ -72,8 +72,87 @@ GlRule gauss_legendre(double b) {
   return r;
 }
 
+// Interpolation weights.  For a point at grid coordinate u = base + W/2 - 1 + f
+// (f in [0, 1)), grid point base + k gets phi((f + W/2 - 1 - k) 2 / W).  Each
+// tap's weight is a polynomial of degree P in z = 2f - 1: the Chebyshev
+// interpolant at P + 1 nodes (FP64 on the host), in monomial form, evaluated by
+// Horner in FP32 with the coefficients as kernel parameters.  Its error is
+// below 1e-7 (W >= 8) -- the FP32 rounding of the weights themselves.
+constexpr int kMaxTaps = 12;
+constexpr int kMaxDegree = 13;
+constexpr int kGridPad = 16;  // periodic extension of each grid row (>= kMaxTaps)
+
+__host__ __device__ constexpr int poly_degree(int W) { return W <= 4 ? 6 : W + 1; }
+
+struct EsPoly {
+  float c[kMaxTaps][kMaxDegree + 1];  // c[k][i]: coefficient of z^i for tap k
+};
+
+double es_kernel(double t, double beta) {
+  return std::exp(beta * (std::sqrt(std::max(0.0, 1.0 - t * t)) - 1.0));
+}
+
+EsPoly es_poly(int W, double beta) {
+  EsPoly e{};
+  const int P = poly_degree(W);
+  const int n = P + 1;
+  for (int k = 0; k < W; ++k) {
+    double val[kMaxDegree + 1], z[kMaxDegree + 1];
+    for (int j = 0; j < n; ++j) {
+      z[j] = std::cos(M_PI * (j + 0.5) / n);
+      const double f = 0.5 * (z[j] + 1.0);
+      val[j] = es_kernel((f + W / 2 - 1 - k) * 2.0 / W, beta);
+    }
+    // Chebyshev coefficients a_i, then sum_i a_i T_i(z) expanded to monomials
+    double mono[kMaxDegree + 1] = {0.0};
+    double t_prev[kMaxDegree + 1] = {0.0}, t_cur[kMaxDegree + 1] = {0.0};
+    t_prev[0] = 1.0;  // T_0
+    t_cur[1] = 1.0;   // T_1
+    for (int i = 0; i < n; ++i) {
+      double a = 0.0;
+      for (int j = 0; j < n; ++j) a += val[j] * std::cos(i * M_PI * (j + 0.5) / n);
+      a *= (i == 0 ? 1.0 : 2.0) / n;
+      const double* ti = i == 0 ? t_prev : t_cur;
+      for (int q = 0; q <= P; ++q) mono[q] += a * ti[q];
+      if (i >= 1) {  // advance: T_{i+1} = 2 z T_i - T_{i-1}
+        double t_next[kMaxDegree + 1] = {0.0};
+        for (int q = 0; q <= P; ++q) {
+          t_next[q] = (q > 0 ? 2.0 * t_cur[q - 1] : 0.0) - t_prev[q];
+        }
+        for (int q = 0; q <= P; ++q) {
+          t_prev[q] = t_cur[q];
+          t_cur[q] = t_next[q];
+        }
+      }
+    }
+    for (int q = 0; q <= P; ++q) e.c[k][q] = static_cast<float>(mono[q]);
+  }
+  return e;
+}
+
+template <int W>
+struct TapWeights {
+  float w[W];
+};
+
+template <int W>
+__device__ __forceinline__ TapWeights<W> tap_weights(const EsPoly& e, float f) {
+  constexpr int P = poly_degree(W);
+  const float z = fmaf(2.0f, f, -1.0f);
+  TapWeights<W> r;
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    float acc = e.c[k][P];
+#pragma unroll
+    for (int i = P - 1; i >= 0; --i) acc = fmaf(acc, z, e.c[k][i]);
+    r.w[k] = acc;
+  }
+  return r;
+}
+
 struct NufftShape {
   int M = 0;      // fine grid points per antenna (power of two)
+  int Mp = 0;     // grid row length in shared / global memory: M + kGridPad
   int log2M = 0;
   int h = 0;      // mode centre, S / 2
   int W = 0;      // kernel width in grid points
@@ -93,15 +172,16 @@ int grid_points(int64_t S) {
 }
 
 // Shared memory of the gather kernel: 2 mbarriers | positions [2][rows][6]
-// double | grid ring [2 stages][re, im][rows][M] float.
+// double | grid ring [2 stages][rows][M + pad] float2.
 size_t gather_buf_off(int rows) { return align256(128 + 2 * static_cast<size_t>(rows) * 6 * sizeof(double)); }
 size_t gather_smem(int rows, int M) {
-  return gather_buf_off(rows) + 4 * static_cast<size_t>(rows) * M * sizeof(float);
+  return gather_buf_off(rows) + 2 * static_cast<size_t>(rows) * (M + kGridPad) * sizeof(float2);
 }
 
 NufftShape nufft_shape(const MfArgs& a, const Tuning& t) {
   NufftShape s;
   s.M = grid_points(a.S);
+  s.Mp = s.M + kGridPad;
   s.log2M = 0;
   while ((1 << s.log2M) < s.M) ++s.log2M;
   s.h = static_cast<int>(a.S / 2);
@@ -114,10 +194,10 @@ NufftShape nufft_shape(const MfArgs& a, const Tuning& t) {
   const int64_t rows_total = (a.A + s.rows - 1) / s.rows;
   const int64_t rows_per_split = (rows_total + s.splits - 1) / s.splits;
   s.ant_per_split = std::max<int64_t>(1, rows_per_split) * s.rows;
-  // workspace: deconvolution factors [S] | grid re/im [2][A][M] | partials [splits][N]
+  // workspace: deconvolution factors [S] | grid [A][M + pad] float2 | partials [splits][N]
   s.deconv_off = 0;
   s.grid_off = align256(static_cast<size_t>(std::max<int64_t>(a.S, 1)) * sizeof(float));
-  s.partial_off = s.grid_off + align256(2 * static_cast<size_t>(a.A) * s.M * sizeof(float));
+  s.partial_off = s.grid_off + align256(static_cast<size_t>(a.A) * s.Mp * sizeof(float2));
   s.total = s.partial_off +
             (s.splits > 1 ? align256(static_cast<size_t>(s.splits) * a.N * sizeof(float2)) : 0);
   s.pos_off = 128;
@@ -157,8 +237,7 @@ struct GridP {
   const T* real;
   const T* imag;
   const float* deconv;
-  float* g_re;  // [A][M]
-  float* g_im;
+  float2* g;  // [A][M + kGridPad]: the M grid points, then the first kGridPad again
   int64_t A;
   int S, h, M, log2M;
 };
@@ -205,23 +284,10 @@ __global__ void __launch_bounds__(512) nufft_grid_kernel(const GridP<T> p) {
     }
     __syncthreads();
     fft_radix2(fbuf, M, -1.0f);
-    for (int l = threadIdx.x; l < M; l += blockDim.x) {
-      const float2 v = fbuf[l];
-      p.g_re[a * M + l] = v.x;
-      p.g_im[a * M + l] = v.y;
-    }
+    const int Mp = M + kGridPad;
+    for (int l = threadIdx.x; l < Mp; l += blockDim.x) p.g[a * Mp + l] = fbuf[l & (M - 1)];
     __syncthreads();
   }
-}
-
-// Interpolation weight of grid point base + k for a point at u = base + W/2 - 1 + f
-// (f in [0, 1)): phi at the offset scaled to [-1, 1].
-template <int W>
-__device__ __forceinline__ float es_weight(float f, int k, float beta_log2e) {
-  constexpr float kInvHalfW = 2.0f / W;
-  const float tt = fmaf(f, kInvHalfW, static_cast<float>(W / 2 - 1 - k) * kInvHalfW);
-  const float one_m = fmaxf(fmaf(-tt, tt, 1.0f), 0.0f);
-  return exp2f(fmaf(beta_log2e, sqrtf(one_m), -beta_log2e));
 }
 
 // Per (voxel, antenna) NUFFT coordinates: the frequency d reduced to [-1/2, 1/2]
@@ -253,12 +319,42 @@ __device__ __forceinline__ NufftPoint nufft_point(double tx, double ty, double t
 }
 
 // ---------------------------------------------------------------------------
+// Double-buffered TMA ring of grid rows (one float2 array): thread 0 issues one
+// cp.async.bulk per stage; completion on the stage's mbarrier, waits bounded.
+struct RowStager {
+  float2* buf;    // [2 stages][rows_max * row]
+  uint64_t* bar;  // [2]
+  int row;        // float2 per row (multiple of 2: 16-byte rows)
+  int rows_max;
+
+  __device__ __forceinline__ float2* stage_ptr(int stage) const {
+    return buf + static_cast<int64_t>(stage) * rows_max * row;
+  }
+  __device__ __forceinline__ void issue(int stage, const float2* src, int64_t row0, int rows) {
+    if (threadIdx.x == 0) {
+      const uint32_t bytes = static_cast<uint32_t>(rows) * row * sizeof(float2);
+      mbar_arrive_expect_tx(&bar[stage], bytes);
+      bulk_g2s(stage_ptr(stage), src + row0 * row, bytes, &bar[stage]);
+    }
+  }
+  __device__ __forceinline__ bool wait(int stage, uint32_t parity, int* status) {
+    const bool ok = mbar_wait_bounded(&bar[stage], parity, status);
+    return __syncthreads_and(ok) != 0;
+  }
+  __device__ __forceinline__ void drain(int stage, uint32_t parity, int* status) {
+    if (threadIdx.x == 0) mbar_wait_bounded(&bar[stage], parity, status);
+  }
+};
+
+// ---------------------------------------------------------------------------
 // 4. Gather: VPT voxels per thread, antenna rows of the fine grid staged by
 // TMA into a double-buffered ring (as the MIXED forward stages IF samples).
+// Each row carries a periodic extension, so a stencil starting at any grid
+// point reads W consecutive entries without wrapping.
 template <typename T>
 struct GatherP {
-  const float* g_re;
-  const float* g_im;
+  EsPoly poly;
+  const float2* g;  // [A][M + kGridPad]
   const T* tx;
   const T* rx;
   const T* voxel;
@@ -269,7 +365,6 @@ struct GatherP {
   int64_t A, N, ant_per_split;
   int M, h, rows, splits;
   double k0, b0, k1, b1;
-  float beta_log2e;  // beta * log2(e)
   size_t pos_off, buf_off;
 };
 
@@ -278,7 +373,8 @@ __global__ void __launch_bounds__(256) nufft_gather_kernel(const GatherP<T> p) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
   double* pos = reinterpret_cast<double*>(smem + p.pos_off);
-  PairStager<float> stg{reinterpret_cast<float*>(smem + p.buf_off), bar, p.M, p.rows, true};
+  const int Mp = p.M + kGridPad;
+  RowStager stg{reinterpret_cast<float2*>(smem + p.buf_off), bar, Mp, p.rows};
 
   const int split = blockIdx.x % p.splits;
   const int64_t vtile = blockIdx.x / p.splits;
@@ -295,15 +391,15 @@ __global__ void __launch_bounds__(256) nufft_gather_kernel(const GatherP<T> p) {
   }
   __syncthreads();
 
-  float vx[VPT], vy[VPT], vz[VPT];
+  double vx[VPT], vy[VPT], vz[VPT];
   int64_t vid[VPT];
 #pragma unroll
   for (int j = 0; j < VPT; ++j) {
     vid[j] = vtile * blockDim.x * VPT + threadIdx.x + static_cast<int64_t>(j) * blockDim.x;
     const bool ok = vid[j] < p.N;
-    vx[j] = ok ? ld_f(p.voxel, vid[j]) : 0.0f;
-    vy[j] = ok ? ld_f(p.voxel, p.N + vid[j]) : 0.0f;
-    vz[j] = ok ? ld_f(p.voxel, 2 * p.N + vid[j]) : 0.0f;
+    vx[j] = ok ? static_cast<double>(ld_f(p.voxel, vid[j])) : 0.0;
+    vy[j] = ok ? static_cast<double>(ld_f(p.voxel, p.N + vid[j])) : 0.0;
+    vz[j] = ok ? static_cast<double>(ld_f(p.voxel, 2 * p.N + vid[j])) : 0.0;
   }
   float yr[VPT], yi[VPT], cr[VPT], ci[VPT];
 #pragma unroll
@@ -312,7 +408,7 @@ __global__ void __launch_bounds__(256) nufft_gather_kernel(const GatherP<T> p) {
   auto issue = [&](int tile, int stage) {
     const int64_t a0 = a_begin + static_cast<int64_t>(tile) * p.rows;
     const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
-    stg.issue(stage, p.g_re, p.g_im, a0, rws, p.M);
+    stg.issue(stage, p.g, a0, rws);
     stage_positions<T, double>(pos, stage, p.rows, p.tx, p.rx, a0, rws);
   };
   if (ntiles > 0) issue(0, 0);
@@ -329,24 +425,19 @@ __global__ void __launch_bounds__(256) nufft_gather_kernel(const GatherP<T> p) {
     for (int r = 0; r < rws; ++r) {
       const double* ps = pos + (s * p.rows + r) * 6;
       const double tx = ps[0], ty = ps[1], tz = ps[2], rx = ps[3], ry = ps[4], rz = ps[5];
-      const float* gre = stg.stage_ptr(s, 0) + r * p.M;
-      const float* gim = stg.stage_ptr(s, 1) + r * p.M;
+      const float2* row = stg.stage_ptr(s) + r * Mp;
 #pragma unroll
       for (int j = 0; j < VPT; ++j) {
-        const NufftPoint q = nufft_point<W>(tx, ty, tz, rx, ry, rz, static_cast<double>(vx[j]),
-                                            static_cast<double>(vy[j]), static_cast<double>(vz[j]),
-                                            p.k0, p.b0, p.k1, p.b1, p.h, fM);
-        float qr = 0.0f, qi = 0.0f;
+        const NufftPoint q = nufft_point<W>(tx, ty, tz, rx, ry, rz, vx[j], vy[j], vz[j], p.k0, p.b0,
+                                            p.k1, p.b1, p.h, fM);
+        const TapWeights<W> wt = tap_weights<W>(p.poly, q.f);
+        const float2* gp = row + (q.base & mask);
+        float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
-        for (int k = 0; k < W; ++k) {
-          const float wt = es_weight<W>(q.f, k, p.beta_log2e);
-          const int l = (q.base + k) & mask;
-          qr = fmaf(wt, gre[l], qr);
-          qi = fmaf(wt, gim[l], qi);
-        }
+        for (int k = 0; k < W; ++k) acc = ffma2(make_float2(wt.w[k], wt.w[k]), gp[k], acc);
         const float2 e = cis_cycles(q.frac);  // e^{+j 2 pi frac}; the forward uses its conjugate
-        const float tr = fmaf(e.x, qr, e.y * qi);
-        const float ti = fmaf(e.x, qi, -e.y * qr);
+        const float tr = fmaf(e.x, acc.x, e.y * acc.y);
+        const float ti = fmaf(e.x, acc.y, -e.y * acc.x);
         kahan_add(yr[j], cr[j], tr);
         kahan_add(yi[j], ci[j], ti);
       }
@@ -406,76 +497,209 @@ cudaError_t launch_deconv(float* deconv, int64_t S, const NufftShape& s, cudaStr
 //   1. spread: f[a, l] = sum_v G_v e^{+j 2 pi (c0 + h d)} phi(u - l) on the fine grid;
 //   2. per antenna an M-point FFT with kernel e^{+j 2 pi m l / M}, then
 //      H[a, m + h] = F(m) / Phi(m / M) / A.
-// Spreading accumulates in shared memory with atomics, so sums are not
-// bit-reproducible from run to run (FP32 rounding level).
+// Spreading.  Per antenna, all voxels fall in a narrow band of grid points
+// (their path lengths lie between the nearest and farthest point of the voxel
+// set's bounding box).  When that band, with the stencil and one point of
+// margin each side, fits kWin grid points, every thread accumulates its voxels
+// into a private column of a [kWin x threads] shared window with plain
+// read-modify-writes, and the columns are summed in a fixed order at the end:
+// no atomics, bit-reproducible results.  Otherwise (bands wider than kWin, or
+// a band that crosses the +-1/2-cycle wrap) the block accumulates into one
+// shared row with FP32 atomics, whose summation order varies from run to run.
+constexpr int kWin = 48;
+constexpr int kSpreadThreads = 128;
+constexpr int kWinLd = kSpreadThreads + 1;  // padded column stride: conflict-free sums
+constexpr int kVoxelsPerThread = 4096;      // per block and antenna: bounds FP32 sums
+constexpr int kStatusInternal = 6;          // GERAF_ERR_DEVICE_CHECK
+
+template <typename T>
+struct BboxP {
+  const T* voxel;  // [3, N]
+  int64_t N;
+  float* partial;  // [blocks][6]
+  float* bbox;     // [6]: lo xyz, hi xyz
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) voxel_bbox_partial_kernel(const BboxP<T> p) {
+  __shared__ float red[6][256];
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < p.N;
+       v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float x = ld_f(p.voxel, c * p.N + v);
+      lo[c] = fminf(lo[c], x);
+      hi[c] = fmaxf(hi[c], x);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    red[c][threadIdx.x] = lo[c];
+    red[3 + c][threadIdx.x] = hi[c];
+  }
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        red[c][threadIdx.x] = fminf(red[c][threadIdx.x], red[c][threadIdx.x + w]);
+        red[3 + c][threadIdx.x] = fmaxf(red[3 + c][threadIdx.x], red[3 + c][threadIdx.x + w]);
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) p.partial[blockIdx.x * 6 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void voxel_bbox_final_kernel(const float* partial, int blocks, float* bbox) {
+  const int c = threadIdx.x;
+  if (c >= 6) return;
+  float r = c < 3 ? INFINITY : -INFINITY;
+  for (int b = 0; b < blocks; ++b) r = c < 3 ? fminf(r, partial[b * 6 + c]) : fmaxf(r, partial[b * 6 + c]);
+  bbox[c] = r;
+}
+
+// Range of path lengths |t - x| + |r - x| over x in the box [lo, hi].
+__device__ __forceinline__ void path_range(const double* t, const double* r, const float* box, double& dlo,
+                                           double& dhi) {
+  double nt = 0.0, nr = 0.0, ft = 0.0, fr = 0.0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double lo = box[c], hi = box[3 + c];
+    const double et = fmax(fmax(lo - t[c], 0.0), t[c] - hi);
+    const double er = fmax(fmax(lo - r[c], 0.0), r[c] - hi);
+    nt += et * et;
+    nr += er * er;
+    const double gt = fmax(fabs(t[c] - lo), fabs(t[c] - hi));
+    const double gr = fmax(fabs(r[c] - lo), fabs(r[c] - hi));
+    ft += gt * gt;
+    fr += gr * gr;
+  }
+  dlo = sqrt(nt) + sqrt(nr);
+  dhi = sqrt(ft) + sqrt(fr);
+}
+
 template <typename T>
 struct SpreadP {
+  EsPoly poly;
   const T* tx;
   const T* rx;
   const T* voxel;
   const T* gr;
   const T* gi;
-  float2* grid;  // [vsplits][A][M]
+  const float* bbox;  // [6]
+  float2* grid;       // [vsplits][A][M]
+  int* status;
   int64_t A, N, vox_per_split;
-  int M, h, rows, vsplits;
+  int M, h, vsplits;
   double k0, b0, k1, b1;
-  float beta_log2e;
-  size_t grid_smem_off;
 };
 
 template <typename T, int W>
-__global__ void __launch_bounds__(256) nufft_spread_kernel(const SpreadP<T> p) {
+__global__ void __launch_bounds__(kSpreadThreads) nufft_spread_kernel(const SpreadP<T> p) {
   extern __shared__ __align__(128) unsigned char smem[];
-  double* pos = reinterpret_cast<double*>(smem);  // [rows][6]
-  float* fre = reinterpret_cast<float*>(smem + p.grid_smem_off);  // [rows][M]
-  float* fim = fre + p.rows * p.M;
+  float* buf = reinterpret_cast<float*>(smem);  // window [2][kWin][kWinLd] or row [2][M]
+  __shared__ double pos[6];
+  __shared__ int s_mode, s_w0;
+  __shared__ float sums[2 * kWin];
   const int vs = blockIdx.x % p.vsplits;
-  const int64_t a0 = static_cast<int64_t>(blockIdx.x / p.vsplits) * p.rows;
-  const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), p.A - a0));
+  const int64_t a = blockIdx.x / p.vsplits;
   const int mask = p.M - 1;
   const float fM = static_cast<float>(p.M);
-  for (int i = threadIdx.x; i < p.rows * p.M; i += blockDim.x) {
-    fre[i] = 0.0f;
-    fim[i] = 0.0f;
+  if (threadIdx.x < 6) {
+    const T* src = threadIdx.x < 3 ? p.tx : p.rx;
+    pos[threadIdx.x] = static_cast<double>(ld_f(src, a * 3 + (threadIdx.x % 3)));
   }
-  stage_positions<T, double>(pos, 0, p.rows, p.tx, p.rx, a0, rws);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double dlo, dhi;
+    path_range(pos, pos + 3, p.bbox, dlo, dhi);
+    double c_lo = fma(dlo, p.k1, p.b1), c_hi = fma(dhi, p.k1, p.b1);
+    if (c_lo > c_hi) {
+      const double tmp = c_lo;
+      c_lo = c_hi;
+      c_hi = tmp;
+    }
+    const double r0 = rint(c_lo);
+    int mode = 0;  // 0: shared row with atomics, 1: private windows
+    int w0 = 0;
+    if (rint(c_hi) == r0 && c_lo - r0 > -0.5 + 1e-6 && c_hi - r0 < 0.5 - 1e-6) {
+      const int b_lo = static_cast<int>(floor((c_lo - r0) * p.M)) - W / 2;      // one point of margin
+      const int b_hi = static_cast<int>(floor((c_hi - r0) * p.M)) - W / 2 + 2;  // one point of margin
+      if (b_hi + W - b_lo <= kWin) {
+        mode = 1;
+        w0 = b_lo;
+      }
+    }
+    s_mode = mode;
+    s_w0 = w0;
+  }
+  __syncthreads();
+  const int mode = s_mode;
+  const int w0 = s_w0;
+  const int cells = mode ? 2 * kWin * kWinLd : 2 * p.M;
+  for (int i = threadIdx.x; i < cells; i += blockDim.x) buf[i] = 0.0f;
   __syncthreads();
 
-  const int lane = threadIdx.x & 31;
   const int64_t v_begin = static_cast<int64_t>(vs) * p.vox_per_split;
   const int64_t v_end = min(p.N, v_begin + p.vox_per_split);
+  float* col_re = buf + threadIdx.x;             // window column of this thread
+  float* col_im = buf + kWin * kWinLd + threadIdx.x;
   for (int64_t v = v_begin + threadIdx.x; v < v_end; v += blockDim.x) {
     const double x = static_cast<double>(ld_f(p.voxel, v));
     const double y = static_cast<double>(ld_f(p.voxel, p.N + v));
     const double z = static_cast<double>(ld_f(p.voxel, 2 * p.N + v));
     const float g_r = ld_f(p.gr, v);
     const float g_i = ld_f(p.gi, v);
-    for (int r = 0; r < rws; ++r) {
-      const double* ps = pos + r * 6;
-      const NufftPoint q = nufft_point<W>(ps[0], ps[1], ps[2], ps[3], ps[4], ps[5], x, y, z, p.k0,
-                                          p.b0, p.k1, p.b1, p.h, fM);
-      const float2 e = cis_cycles(q.frac);
-      const float wr = fmaf(g_r, e.x, -g_i * e.y);
-      const float wi = fmaf(g_r, e.y, g_i * e.x);
-      float* rre = fre + r * p.M;
-      float* rim = fim + r * p.M;
-      // Lanes start at different taps so that neighbouring voxels (which share
-      // most of their stencil) hit different grid points in each step.
+    const NufftPoint q = nufft_point<W>(pos[0], pos[1], pos[2], pos[3], pos[4], pos[5], x, y, z, p.k0,
+                                        p.b0, p.k1, p.b1, p.h, fM);
+    const float2 e = cis_cycles(q.frac);
+    const float wr = fmaf(g_r, e.x, -g_i * e.y);
+    const float wi = fmaf(g_r, e.y, g_i * e.x);
+    const TapWeights<W> wt = tap_weights<W>(p.poly, q.f);
+    if (mode) {
+      const int o = q.base - w0;
+      if (static_cast<unsigned>(o) > static_cast<unsigned>(kWin - W)) {
+        // outside the band bound from the bounding box: cannot happen for finite inputs
+        if (p.status != nullptr) atomicExch(p.status, kStatusInternal);
+        continue;
+      }
 #pragma unroll
       for (int k = 0; k < W; ++k) {
-        const int kk = (k + lane) % W;
-        const float wt = es_weight<W>(q.f, kk, p.beta_log2e);
-        const int l = (q.base + kk) & mask;
-        atomicAdd(rre + l, wt * wr);
-        atomicAdd(rim + l, wt * wi);
+        col_re[(o + k) * kWinLd] += wt.w[k] * wr;
+        col_im[(o + k) * kWinLd] += wt.w[k] * wi;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        const int l = (q.base + k) & mask;
+        atomicAdd(buf + l, wt.w[k] * wr);
+        atomicAdd(buf + p.M + l, wt.w[k] * wi);
       }
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < rws * p.M; i += blockDim.x) {
-    const int r = i / p.M;
-    const int l = i - r * p.M;
-    p.grid[(static_cast<int64_t>(vs) * p.A + a0 + r) * p.M + l] = make_float2(fre[i], fim[i]);
+  float2* out = p.grid + (static_cast<int64_t>(vs) * p.A + a) * p.M;
+  if (mode) {
+    if (threadIdx.x < 2 * kWin) {
+      const float* rowp = buf + threadIdx.x * kWinLd;
+      float acc = 0.0f;
+      for (int t = 0; t < kSpreadThreads; ++t) acc += rowp[t];
+      sums[threadIdx.x] = acc;
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l < p.M; l += blockDim.x) {
+      // window points j and j + M are the same grid point when M < kWin
+      float2 v = make_float2(0.0f, 0.0f);
+      for (int j = (l - w0) & mask; j < kWin; j += p.M) {
+        v.x += sums[j];
+        v.y += sums[kWin + j];
+      }
+      out[l] = v;
+    }
+  } else {
+    for (int l = threadIdx.x; l < p.M; l += blockDim.x) out[l] = make_float2(buf[l], buf[p.M + l]);
   }
 }
 
@@ -528,16 +752,18 @@ const void* spread_kernel_ptr(int W) {
   }
 }
 
-size_t spread_grid_off(int rows) { return align256(static_cast<size_t>(rows) * 6 * sizeof(double)); }
-size_t spread_smem(int rows, int M) {
-  return spread_grid_off(rows) + 2 * static_cast<size_t>(rows) * M * sizeof(float);
+// Dynamic shared memory of the spread kernel: the private windows or the
+// fallback row, whichever is larger.
+size_t spread_smem(int M) {
+  return std::max(2 * static_cast<size_t>(kWin) * kWinLd, 2 * static_cast<size_t>(M)) * sizeof(float);
 }
+constexpr int kBboxBlocks = 256;
 
 struct AdjShape {
   NufftShape base;
   int vsplits = 1;
   int64_t vox_per_split = 0;
-  size_t deconv_off = 0, grid_off = 0, total = 0;
+  size_t deconv_off = 0, bbox_off = 0, grid_off = 0, total = 0;
 };
 
 AdjShape adj_shape(const MfArgs& a, const Tuning& t) {
@@ -545,8 +771,10 @@ AdjShape adj_shape(const MfArgs& a, const Tuning& t) {
   s.base = nufft_shape(a, t);
   s.vsplits = t.splits;
   s.vox_per_split = std::max<int64_t>(1, (a.N + s.vsplits - 1) / s.vsplits);
+  // workspace: deconvolution [S] | bbox partials [kBboxBlocks][6] + bbox [6] | grids [vsplits][A][M]
   s.deconv_off = 0;
-  s.grid_off = align256(static_cast<size_t>(std::max<int64_t>(a.S, 1)) * sizeof(float));
+  s.bbox_off = align256(static_cast<size_t>(std::max<int64_t>(a.S, 1)) * sizeof(float));
+  s.grid_off = s.bbox_off + align256((kBboxBlocks + 1) * 6 * sizeof(float));
   s.total = s.grid_off + align256(static_cast<size_t>(s.vsplits) * a.A * s.base.M * sizeof(float2));
   return s;
 }
@@ -562,36 +790,50 @@ cudaError_t launch_nufft_backward(const MfArgs& a, const Tuning& t, void* ws, cu
   cudaError_t err = launch_deconv(deconv, a.S, b, st);
   if (err != cudaSuccess) return err;
 
+  float* bbox_partial = reinterpret_cast<float*>(base + s.bbox_off);
+  float* bbox = bbox_partial + kBboxBlocks * 6;
+  if (a.N > 0) {
+    BboxP<T> bp;
+    bp.voxel = static_cast<const T*>(a.voxel);
+    bp.N = a.N;
+    bp.partial = bbox_partial;
+    bp.bbox = bbox;
+    const int nb = static_cast<int>(std::min<int64_t>(kBboxBlocks, (a.N + 255) / 256));
+    voxel_bbox_partial_kernel<T><<<nb, 256, 0, st>>>(bp);
+    voxel_bbox_final_kernel<<<1, 32, 0, st>>>(bbox_partial, nb, bbox);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+  }
+
   SpreadP<T> sp;
+  sp.poly = es_poly(b.W, b.beta);
   sp.tx = static_cast<const T*>(a.tx);
   sp.rx = static_cast<const T*>(a.rx);
   sp.voxel = static_cast<const T*>(a.voxel);
   sp.gr = static_cast<const T*>(a.grad_real_out);
   sp.gi = static_cast<const T*>(a.grad_imag_out);
+  sp.bbox = bbox;
   sp.grid = grid;
+  sp.status = device_status_ptr();
   sp.A = a.A;
   sp.N = a.N;
   sp.vox_per_split = s.vox_per_split;
   sp.M = b.M;
   sp.h = b.h;
-  sp.rows = t.stage_rows;
   sp.vsplits = s.vsplits;
   const PhaseConsts pc = phase_consts(kMfStartFrequency, a.As, a.fs);
   sp.k0 = pc.k0;
   sp.b0 = pc.b0;
   sp.k1 = pc.k1;
   sp.b1 = pc.b1;
-  sp.beta_log2e = static_cast<float>(b.beta * 1.4426950408889634);
-  sp.grid_smem_off = spread_grid_off(t.stage_rows);
-  const size_t ssmem = spread_smem(t.stage_rows, b.M);
+  const size_t ssmem = spread_smem(b.M);
   const void* fn = spread_kernel_ptr<T>(b.W);
   err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(ssmem));
   if (err != cudaSuccess) return err;
-  const int64_t atiles = (a.A + t.stage_rows - 1) / t.stage_rows;
-  const int64_t blocks = atiles * s.vsplits;
+  const int64_t blocks = a.A * s.vsplits;
   if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
   void* args[] = {&sp};
-  err = cudaLaunchKernel(fn, dim3(static_cast<unsigned>(blocks)), dim3(t.threads), args, ssmem, st);
+  err = cudaLaunchKernel(fn, dim3(static_cast<unsigned>(blocks)), dim3(kSpreadThreads), args, ssmem, st);
   if (err != cudaSuccess) return err;
 
   AdjFftP<T> fp;
@@ -620,8 +862,7 @@ template <typename T>
 cudaError_t launch_nufft_forward(const MfArgs& a, const NufftShape& s, void* ws, cudaStream_t st) {
   unsigned char* base = static_cast<unsigned char*>(ws);
   float* deconv = reinterpret_cast<float*>(base + s.deconv_off);
-  float* g_re = reinterpret_cast<float*>(base + s.grid_off);
-  float* g_im = g_re + static_cast<size_t>(a.A) * s.M;
+  float2* grid = reinterpret_cast<float2*>(base + s.grid_off);
   const DeviceInfo dev = current_device_info();
 
   if (a.S > 0) {
@@ -632,8 +873,7 @@ cudaError_t launch_nufft_forward(const MfArgs& a, const NufftShape& s, void* ws,
     gp.real = static_cast<const T*>(a.real);
     gp.imag = static_cast<const T*>(a.imag);
     gp.deconv = deconv;
-    gp.g_re = g_re;
-    gp.g_im = g_im;
+    gp.g = grid;
     gp.A = a.A;
     gp.S = static_cast<int>(a.S);
     gp.h = s.h;
@@ -652,13 +892,13 @@ cudaError_t launch_nufft_forward(const MfArgs& a, const NufftShape& s, void* ws,
     }
   } else if (a.A > 0) {
     // No samples: every grid point is zero.
-    cudaError_t err = cudaMemsetAsync(g_re, 0, 2 * static_cast<size_t>(a.A) * s.M * sizeof(float), st);
+    cudaError_t err = cudaMemsetAsync(grid, 0, static_cast<size_t>(a.A) * s.Mp * sizeof(float2), st);
     if (err != cudaSuccess) return err;
   }
 
   GatherP<T> p;
-  p.g_re = g_re;
-  p.g_im = g_im;
+  p.poly = es_poly(s.W, s.beta);
+  p.g = grid;
   p.tx = static_cast<const T*>(a.tx);
   p.rx = static_cast<const T*>(a.rx);
   p.voxel = static_cast<const T*>(a.voxel);
@@ -678,7 +918,6 @@ cudaError_t launch_nufft_forward(const MfArgs& a, const NufftShape& s, void* ws,
   p.b0 = pc.b0;
   p.k1 = pc.k1;
   p.b1 = pc.b1;
-  p.beta_log2e = static_cast<float>(s.beta * 1.4426950408889634);
   p.pos_off = s.pos_off;
   p.buf_off = s.buf_off;
 
@@ -708,7 +947,7 @@ Tuning mf_nufft_forward_resolve(const MfArgs& a, const Tuning& req) {
   if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 128;
   if (t.items != 1 && t.items != 2 && t.items != 4) t.items = 4;
   if (t.taps != 4 && t.taps != 6 && t.taps != 8 && t.taps != 10 && t.taps != 12) t.taps = 8;
-  if (t.stage_rows <= 0) t.stage_rows = 8;
+  if (t.stage_rows <= 0) t.stage_rows = 4;
   t.stage_rows = std::min(t.stage_rows, 64);
   const int M = grid_points(a.S);
   const DeviceInfo dev = current_device_info();
@@ -731,23 +970,19 @@ bool mf_nufft_supported(int64_t S) { return S <= kNufftMaxSamples; }
 
 Tuning mf_nufft_backward_resolve(const MfArgs& a, const Tuning& req) {
   Tuning t = req;
-  if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 256;
+  // one block of kSpreadThreads per (antenna, voxel split)
+  t.threads = kSpreadThreads;
   if (t.taps != 4 && t.taps != 6 && t.taps != 8 && t.taps != 10 && t.taps != 12) t.taps = 8;
   t.items = 1;
-  if (t.stage_rows <= 0) t.stage_rows = 8;
-  t.stage_rows = std::min(t.stage_rows, 64);
-  const int M = grid_points(a.S);
-  const DeviceInfo dev = current_device_info();
-  while (t.stage_rows > 1 && spread_smem(t.stage_rows, M) > static_cast<size_t>(dev.max_smem_optin)) {
-    t.stage_rows /= 2;
-  }
-  // voxel splits: enough antenna-tile x voxel-range blocks to fill the GPU,
-  // with at least 2048 voxels per block
-  const int64_t atiles = std::max<int64_t>(1, (a.A + t.stage_rows - 1) / t.stage_rows);
-  const int64_t max_vs = std::max<int64_t>(1, a.N / 2048);
+  t.stage_rows = 1;
+  // voxel splits: at most kVoxelsPerThread voxels per thread and block, and
+  // enough (antenna, split) blocks to fill the GPU
+  const int64_t min_vs = std::max<int64_t>(
+      1, (a.N + int64_t{kSpreadThreads} * kVoxelsPerThread - 1) / (int64_t{kSpreadThreads} * kVoxelsPerThread));
+  const int64_t max_vs = std::max<int64_t>(min_vs, a.N / (4 * kSpreadThreads));
   if (t.splits <= 0) {
-    const int per_sm = std::max(1, 1024 / t.threads);
-    t.splits = pick_splits(atiles, per_sm, dev.sm_count, max_vs);
+    const DeviceInfo dev = current_device_info();
+    t.splits = std::max<int>(static_cast<int>(min_vs), pick_splits(std::max<int64_t>(1, a.A), 4, dev.sm_count, max_vs));
   }
   t.splits = static_cast<int>(std::min<int64_t>(std::max(t.splits, 1), std::max<int64_t>(1, a.N)));
   return t;

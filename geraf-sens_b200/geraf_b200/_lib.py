@@ -19,6 +19,7 @@ GERAF_ERR_UNSUPPORTED = 2
 GERAF_ERR_WORKSPACE = 3
 GERAF_ERR_CUDA = 4
 GERAF_ERR_DEVICE_TIMEOUT = 5
+GERAF_ERR_DEVICE_CHECK = 6
 
 DTYPE_F32 = 0
 DTYPE_F64 = 1

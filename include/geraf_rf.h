@@ -41,6 +41,7 @@ extern "C" {
 #define GERAF_ERR_WORKSPACE 3        /* workspace missing, short or misaligned   */
 #define GERAF_ERR_CUDA 4             /* a CUDA runtime call or launch failed      */
 #define GERAF_ERR_DEVICE_TIMEOUT 5   /* a bounded device-side wait gave up        */
+#define GERAF_ERR_DEVICE_CHECK 6     /* a device-side consistency check failed    */
 
 /* ---- element types (match the reference's AT_DISPATCH lists) ----------- */
 #define GERAF_DTYPE_F32 0
@@ -88,15 +89,18 @@ int32_t geraf_rf_cudart_version(void);
  * (reference: csrc/vision.cpp:47-68, get_compiler_version). */
 const char* geraf_rf_build_info(void);
 /* Measures nothing itself: enqueues blocks x threads threads (threads <= 256)
- * of `iters` iterations of 8 independent FP32 FMAs, i.e. blocks*threads*iters*16
- * flops, for timing by the caller.  `sink` is device memory of blocks*threads
+ * of `iters` iterations of 8 independent packed FP32 FMAs (2 FMAs each), i.e.
+ * blocks*threads*iters*32 flops, for timing by the caller.  `sink` is device memory of blocks*threads
  * floats (never written in practice).  The FP32-pipe roofline denominator of
  * the RF kernels; no counterpart in the reference. */
 int32_t geraf_rf_fma_probe(int32_t blocks, int32_t threads, int32_t iters, float* sink,
                            void* stream);
 /* Reads, and with reset != 0 clears, the device status word of the current
- * device (GERAF_OK or GERAF_ERR_DEVICE_TIMEOUT raised by a bounded wait inside
- * a kernel).  Synchronises `stream`. */
+ * device: GERAF_OK, or the code a kernel raised -- GERAF_ERR_DEVICE_TIMEOUT
+ * (a bounded wait gave up), GERAF_ERR_INVALID_ARGUMENT (malformed ragged
+ * point offsets), GERAF_ERR_DEVICE_CHECK (a NUFFT adjoint point fell outside
+ * the band bounded from the voxels' bounding box; it was skipped).
+ * Synchronises `stream`. */
 int32_t geraf_rf_device_status(void* stream, int32_t reset, int32_t* status_out);
 
 /* ---- RFMatchedFilter ---------------------------------------------------- */

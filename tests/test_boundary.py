@@ -80,17 +80,17 @@ def test_workspace_query_without_gpu():
     t = _lib.Tuning.from_dict({"splits": 4})
     n = _lib.workspace_bytes("geraf_mf_forward_workspace_bytes", 64, 32, 1000, 0, 1, ctypes.byref(t))
     assert n == 4 * 1000 * 8
-    # NUFFT: deconvolution factors (S floats, 256-aligned) + the [2][A][M] range grid
-    # (M = 64 for S = 32), plus [splits][N] partials / [splits][A][M] adjoint grids.
+    # NUFFT: deconvolution factors (S floats, 256-aligned) + the [A][M + 16] float2 range
+    # grid (M = 64 for S = 32), plus [splits][N] partials / [splits][A][M] adjoint grids.
     t = _lib.Tuning.from_dict({"splits": 1})
     n = _lib.workspace_bytes("geraf_mf_forward_workspace_bytes", 64, 32, 1000, 0, _lib.MODE_NUFFT, ctypes.byref(t))
-    assert n == 256 + 2 * 64 * 64 * 4
+    assert n == 256 + 64 * 80 * 8
     t = _lib.Tuning.from_dict({"splits": 3})
     n = _lib.workspace_bytes("geraf_mf_forward_workspace_bytes", 64, 32, 1000, 0, _lib.MODE_NUFFT, ctypes.byref(t))
-    assert n == 256 + 2 * 64 * 64 * 4 + 24064  # 3 * 1000 float2, 256-aligned
+    assert n == 256 + 64 * 80 * 8 + 24064  # 3 * 1000 float2, 256-aligned
     n = _lib.workspace_bytes("geraf_mf_backward_workspace_bytes", 64, 32, 1000, 0, _lib.MODE_NUFFT,
                              ctypes.byref(t))
-    assert n == 256 + 3 * 64 * 64 * 8
+    assert n == 256 + 6400 + 3 * 64 * 64 * 8  # + voxel bounding-box scratch (257 x 6 floats)
     lib = _lib.load()
     size = ctypes.c_size_t(0)
     rc = lib.geraf_mf_forward_workspace_bytes(4, 5000, 10, 0, _lib.MODE_NUFFT, None, ctypes.byref(size))

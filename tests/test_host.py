@@ -162,3 +162,28 @@ def test_sarimage_roundtrip_and_sampling(tmp_path):
     pts = torch.tensor([[-1.0, -1.0, -1.0], [1.0, 1.0, 1.0], [1.0, -1.0, 1.0]])
     got = volume.sample_volume(vol, pts)
     assert torch.allclose(got, torch.tensor([vol[0, 0, 0], vol[3, 2, 4], vol[3, 0, 4]]))
+
+
+def test_stage1_eval_geometry_helpers():
+    """Surface samples lie on the analytic cube + torus, the grid zero-crossing
+    extractor recovers a sphere, and the Chamfer distance behaves as a metric."""
+    from geraf_b200 import stage1_eval as ev
+
+    rng = np.random.default_rng(0)
+    pts = ev.analytic_surface_points(4000, rng).astype(np.float64) - np.array([0.0, 0.0, 0.4])
+    on_cube = np.isclose(np.abs(pts).max(1), 0.15, atol=1e-6)
+    rho = np.hypot(pts[:, 0], pts[:, 1])
+    on_torus = np.isclose((rho - 0.08) ** 2 + pts[:, 2] ** 2, 0.03 ** 2, atol=1e-7)
+    assert np.all(on_cube | on_torus) and on_cube.any() and on_torus.any()
+
+    center = torch.tensor([0.0, 0.0, 0.4])
+
+    def sphere(x):  # normalised coordinates, radius 0.5 -> 0.1 m at scale 0.2
+        return x.norm(dim=-1, keepdim=True) - 0.5, None
+
+    surf = ev.sdf_surface_points(sphere, center, 0.2, res=48)
+    radius = (surf - center).norm(dim=-1)
+    assert surf.shape[0] > 1000 and torch.allclose(radius, torch.full_like(radius, 0.1), atol=2e-4)
+    a = torch.tensor(rng.standard_normal((300, 3)), dtype=torch.float32)
+    assert ev.chamfer(a, a) == 0.0
+    assert ev.chamfer(a, a + torch.tensor([0.01, 0.0, 0.0])) > 0.0
