@@ -95,3 +95,30 @@ def test_model_reproduces_oracle_matched_filter():
         y += np.exp(-2j * np.pi * (c0 - np.rint(c0))) * nufft_sum(s[a], d, 10)
     y /= tx.shape[0]
     assert rel_l2(y, ref) < 1e-6
+
+
+# degree of each tap's weight polynomial (nufft_kernels.cu, poly_degree) and its bound
+POLY = {4: (5, 1e-4), 6: (6, 3e-6), 8: (7, 1.5e-7), 10: (9, 1.5e-7), 12: (11, 1.5e-7)}
+
+
+@pytest.mark.parametrize("W", sorted(POLY))
+def test_tap_weight_polynomials(W):
+    """Chebyshev interpolants of the tap weights at P + 1 nodes, in monomial form,
+    evaluated by FP32 Horner, stay within the stated absolute error."""
+    from numpy.polynomial import chebyshev as C
+
+    P, bound = POLY[W]
+    beta = 2.30 * W
+    nodes = np.cos(np.pi * (np.arange(P + 1) + 0.5) / (P + 1))
+    f = np.linspace(0.0, 1.0, 20001)[:-1]
+    z32 = (2.0 * f - 1.0).astype(np.float32)
+    worst = 0.0
+    for k in range(W):
+        def w(zz):
+            return es(((zz + 1.0) / 2.0 + W / 2 - 1 - k) * 2.0 / W, beta)
+        mono = C.cheb2poly(C.chebfit(nodes, w(nodes), P)).astype(np.float32)
+        acc = np.full_like(z32, mono[-1])
+        for c in mono[-2::-1]:
+            acc = acc * z32 + c
+        worst = max(worst, float(np.abs(acc.astype(np.float64) - w(2.0 * f - 1.0)).max()))
+    assert worst < bound
