@@ -456,9 +456,11 @@ def _stage1_extra(args, dev) -> dict:
     res = {}
     vox = torch.tensor(scenes.voxel_grid(128, size=0.32).T.copy(), device=dev)
     target = torch.ones(vox.shape[0], device=dev)
-    for name, prec, graph, iters in (("mixed_graph", "mixed", True, 5), ("plain_eager", "plain", False, 1)):
+    for name, prec, mf_prec, graph, iters in (("mixed_graph", "mixed", "mixed", True, 5),
+                                              ("mixed_nufft_mf_graph", "mixed", "nufft", True, 5),
+                                              ("plain_eager", "plain", "plain", False, 1)):
         st = Stage1RFStep(num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=256, voxels=vox,
-                          target_mag=target, precision=prec, device=dev, seed=args.seed)
+                          target_mag=target, precision=prec, device=dev, seed=args.seed, mf_precision=mf_prec)
         if graph:
             st.capture()
         ms = autotune.time_call(st.run, iters=iters, warmup=1)

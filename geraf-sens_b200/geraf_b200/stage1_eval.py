@@ -129,6 +129,8 @@ def train(precision: str, graph: bool, steps: int, seed: int = 0, voxels_per_axi
     st = Stage1RFStep(num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=256, voxels=vox,
                       precision=precision, device=dev, seed=seed)
     st.target = scene_target(st, seed)
+    ref = torch.tensor(analytic_surface_points(20000, np.random.default_rng(seed + 7)), device=dev)
+    sdf_init = sdf_on_surface(st.net, st.center, st.scale, ref)
     if graph:
         st.capture()
     # a fixed schedule of ray resamplings, identical for both forms
@@ -142,11 +144,12 @@ def train(precision: str, graph: bool, steps: int, seed: int = 0, voxels_per_axi
     torch.cuda.synchronize()
     secs = time.perf_counter() - t0
     surf = sdf_surface_points(st.net, st.center, st.scale)
-    ref = torch.tensor(analytic_surface_points(20000, np.random.default_rng(seed + 7)), device=dev)
     loss = torch.stack(losses).cpu().numpy()
     return {"precision": precision, "graph": graph, "steps": steps, "ms_per_step": 1e3 * secs / steps,
             "it_per_s": steps / secs, "loss_first": float(loss[0]), "loss_last": float(loss[-1]),
+            "loss_every_10": [float(v) for v in loss[::10]],
             "chamfer_m": chamfer(surf, ref), "surface_points": int(surf.shape[0]),
+            "sdf_on_surface_init_m": sdf_init,
             "sdf_on_surface_m": sdf_on_surface(st.net, st.center, st.scale, ref)}
 
 

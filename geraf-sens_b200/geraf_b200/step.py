@@ -13,8 +13,9 @@ Two step shapes that a GeRaF training loop runs:
   gradient, differentiable) and amplitudes (alpha-composited weights x
   reflectance); the tracer renders the IF of a bank of antennas from the shared
   points, the matched filter images it onto target voxels, an L1 loss on the
-  magnitude against a target volume is back-propagated (double backward
-  through the SDF gradient) and Adam updates the network.
+  magnitude against a target volume, plus the eikonal regulariser on the SDF
+  gradient, is back-propagated (double backward through the SDF gradient) and
+  Adam updates the network.
 
 ``capture()`` records one whole step (forward, backward and, for the stage-1
 step, the optimizer update) into a CUDA graph over static input buffers;
@@ -101,13 +102,19 @@ class Stage1RFStep(_Graphable):
     """A stage-1 GeRaF RF step with a random-init NeuS SDF MLP (see ``geraf_b200.sdf``)."""
 
     def __init__(self, num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=128, voxels=None,
-                 target_mag=None, precision: str = "mixed", device="cuda", seed=0, lr=5e-4):
+                 target_mag=None, precision: str = "mixed", device="cuda", seed=0, lr=5e-4,
+                 mf_precision: str | None = None, grad_regression: float = 0.1):
         from . import scenes
         from .sdf import SDFNetwork
 
         torch.manual_seed(seed)
         self.device = torch.device(device)
         self.precision = precision
+        # the matched filter may run a form of its own ("nufft"); the tracer runs `precision`
+        self.mf_precision = mf_precision or precision
+        # eikonal regulariser weight (the reference's `with_grad_regression`, 0.1 in
+        # configs/geraf/bunnyboxv1/geraf2_bunnyboxv1_stage1.py:62)
+        self.grad_regression = grad_regression
         self.net = SDFNetwork().to(self.device)
         self.head = nn.Linear(256, 1).to(self.device)
         self.log_inv_s = nn.Parameter(torch.tensor(10 * 0.3, device=self.device))  # inv_s = e^3
@@ -172,9 +179,12 @@ class Stage1RFStep(_Graphable):
                                     self.inbounds, S, self.cfg["adcSampleRate"], self.cfg["fc_start"],
                                     self.cfg["As_sci"], A, P, precision=self.precision)
         yr, yi = matched_filter_cuda(xr, xi, self.tx, self.rx, self.voxels, A, S, self.cfg["adcSampleRate"],
-                                     self.cfg["As_sci"], self.voxels.shape[0], precision=self.precision)
+                                     self.cfg["As_sci"], self.voxels.shape[0], precision=self.mf_precision)
         mag = torch.sqrt(yr * yr + yi * yi + 1e-20)
         loss = (mag / (mag.detach().mean() + 1e-20) - self.target).abs().mean()
+        if self.grad_regression:
+            # mean (|grad sdf| - 1)^2 over the samples (rf_rendering.py:647-650, 818-819)
+            loss = loss + self.grad_regression * ((grad.norm(dim=-1) - 1.0) ** 2).mean()
         loss.backward()
         self.opt.step()
         return loss.detach()
