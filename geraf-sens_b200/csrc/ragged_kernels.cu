@@ -331,20 +331,18 @@ __global__ void __launch_bounds__(128) ragged_bwd_kernel(const RgP<T> p, int ld,
       const PhaseCycles pc = path_cycles(txp[0] - px, txp[1] - py, txp[2] - pz, rxp[0] - px,
                                          rxp[1] - py, rxp[2] - pz, p.k0, p.b0, p.k1, p.b1);
       const float2 zt = cis_cycles(pc.dcyc);
-      // X = (d_re, q_re), Y = (d_im, q_im): the two recurrences in packed pairs
-      // (the derivative pair is only formed when position gradients are wanted).
-      float2 X = make_float2(0.0f, 0.0f), Y = make_float2(0.0f, 0.0f);
-      const float2 ZX = make_float2(zt.x, zt.x), ZY = make_float2(zt.y, zt.y);
-      const float2 NZY = make_float2(-zt.y, -zt.y);
+      float qr = 0.0f, qi = 0.0f, dr = 0.0f, di = 0.0f;
       auto step = [&](float cr, float ci) {
         if (WITH_POINTS) {
-          horner_dq_step(X, Y, ZX, ZY, NZY, cr, ci);
-        } else {
-          const float nqr = fmaf(X.y, zt.x, fmaf(-Y.y, zt.y, cr));
-          const float nqi = fmaf(X.y, zt.y, fmaf(Y.y, zt.x, -ci));
-          X.y = nqr;
-          Y.y = nqi;
+          const float ndr = fmaf(dr, zt.x, fmaf(-di, zt.y, qr));
+          const float ndi = fmaf(dr, zt.y, fmaf(di, zt.x, qi));
+          dr = ndr;
+          di = ndi;
         }
+        const float nqr = fmaf(qr, zt.x, fmaf(-qi, zt.y, cr));
+        const float nqi = fmaf(qr, zt.y, fmaf(qi, zt.x, -ci));
+        qr = nqr;
+        qi = nqi;
       };
       if (staged) {
         const float* rr = srow + ((a - a0) * 2 + 0) * ld;
@@ -360,7 +358,6 @@ __global__ void __launch_bounds__(128) ragged_bwd_kernel(const RgP<T> p, int ld,
       } else {
         for (int64_t n = p.S - 1; n >= 0; --n) step(ld_f(p.gr, a * p.S + n), ld_f(p.gi, a * p.S + n));
       }
-      const float dr = X.x, qr = X.y, di = Y.x, qi = Y.y;
       const float inv_pa = 1.0f / static_cast<float>(p.offsets[a + 1] - p.offsets[a]);
       const float2 e0 = cis_cycles(pc.frac0);
       const float sum_re = cmul(e0, make_float2(qr, qi)).x;

@@ -149,20 +149,5 @@ __device__ __forceinline__ float adjoint_phase_rate<float>(float f0, float As, f
   return __fmaf_rn(phase_slope, sample_time, phase_base);
 }
 
-// One step of the adjoint's two Horner recurrences over conj(g):
-//   d <- d zeta + q   (derivative sum, uses q before its update)
-//   q <- q zeta + (cr - j ci)
-// on packed pairs X = (d_re, q_re), Y = (d_im, q_im) with ZX = (zeta_re, zeta_re),
-// ZY = (zeta_im, zeta_im), NZY = -ZY: four packed FMAs give exactly the
-// roundings of the eight scalar fmaf of the two recurrences.
-__device__ __forceinline__ void horner_dq_step(float2& X, float2& Y, float2 ZX, float2 ZY, float2 NZY,
-                                               float cr, float ci) {
-  const float2 t1 = ffma2(Y, NZY, make_float2(X.y, cr));
-  const float2 t2 = ffma2(Y, ZX, make_float2(Y.y, -ci));
-  const float2 nx = ffma2(X, ZX, t1);
-  Y = ffma2(X, ZY, t2);
-  X = nx;
-}
-
 }  // namespace tracer
 }  // namespace geraf

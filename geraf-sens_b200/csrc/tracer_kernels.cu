@@ -525,37 +525,24 @@ __global__ void __launch_bounds__(128) tracer_bwd_mixed_kernel(const TrP<T> p) {
       const T* rowi = stg.stage_ptr(s, 1) + r * p.ld;
       // Horner with c_n = conj(g_n): q <- q zeta + c_n;  d <- d zeta + q (before q's update).
       float qr = 0.0f, qi = 0.0f, dr = 0.0f, di = 0.0f;
-      if (WITH_POINTS) {
-        float2 X = make_float2(0.0f, 0.0f), Y = make_float2(0.0f, 0.0f);
-        const float2 ZX = make_float2(zt.x, zt.x), ZY = make_float2(zt.y, zt.y);
-        const float2 NZY = make_float2(-zt.y, -zt.y);
 #pragma unroll 2
-        for (int n = p.ld - 4; n >= 0; n -= 4) {
-          const float4 a4 = lds4(rowr + n);
-          const float4 b4 = lds4(rowi + n);
-          horner_dq_step(X, Y, ZX, ZY, NZY, a4.w, b4.w);
-          horner_dq_step(X, Y, ZX, ZY, NZY, a4.z, b4.z);
-          horner_dq_step(X, Y, ZX, ZY, NZY, a4.y, b4.y);
-          horner_dq_step(X, Y, ZX, ZY, NZY, a4.x, b4.x);
-        }
-        dr = X.x;
-        qr = X.y;
-        di = Y.x;
-        qi = Y.y;
-      } else {
-#pragma unroll 2
-        for (int n = p.ld - 4; n >= 0; n -= 4) {
-          const float4 a4 = lds4(rowr + n);
-          const float4 b4 = lds4(rowi + n);
-          const float cr[4] = {a4.w, a4.z, a4.y, a4.x};
-          const float cim[4] = {b4.w, b4.z, b4.y, b4.x};
+      for (int n = p.ld - 4; n >= 0; n -= 4) {
+        const float4 a4 = lds4(rowr + n);
+        const float4 b4 = lds4(rowi + n);
+        const float cr[4] = {a4.w, a4.z, a4.y, a4.x};
+        const float cim[4] = {b4.w, b4.z, b4.y, b4.x};
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const float nqr = fmaf(qr, zt.x, fmaf(-qi, zt.y, cr[q]));
-            const float nqi = fmaf(qr, zt.y, fmaf(qi, zt.x, -cim[q]));
-            qr = nqr;
-            qi = nqi;
+        for (int q = 0; q < 4; ++q) {
+          if (WITH_POINTS) {
+            const float ndr = fmaf(dr, zt.x, fmaf(-di, zt.y, qr));
+            const float ndi = fmaf(dr, zt.y, fmaf(di, zt.x, qi));
+            dr = ndr;
+            di = ndi;
           }
+          const float nqr = fmaf(qr, zt.x, fmaf(-qi, zt.y, cr[q]));
+          const float nqi = fmaf(qr, zt.y, fmaf(qi, zt.x, -cim[q]));
+          qr = nqr;
+          qi = nqi;
         }
       }
       const float2 e0 = cis_cycles(pc.frac0);
