@@ -137,17 +137,27 @@ struct TapWeights {
   float w[W];
 };
 
+// phi is even, so tap W-1-k at z is tap k at -z: with tap k's polynomial split
+// into even and odd parts E_k(z^2) + z O_k(z^2), the mirror pair is E_k + z O_k
+// and E_k - z O_k -- one evaluation for two taps.
 template <int W>
 __device__ __forceinline__ TapWeights<W> tap_weights(const EsPoly& e, float f) {
   constexpr int P = poly_degree(W);
+  constexpr int PE = P & ~1;        // highest even power
+  constexpr int PO = (P - 1) | 1;   // highest odd power
   const float z = fmaf(2.0f, f, -1.0f);
+  const float z2 = z * z;
   TapWeights<W> r;
 #pragma unroll
-  for (int k = 0; k < W; ++k) {
-    float acc = e.c[k][P];
+  for (int k = 0; k < W / 2; ++k) {
+    float ev = e.c[k][PE];
 #pragma unroll
-    for (int i = P - 1; i >= 0; --i) acc = fmaf(acc, z, e.c[k][i]);
-    r.w[k] = acc;
+    for (int i = PE - 2; i >= 0; i -= 2) ev = fmaf(ev, z2, e.c[k][i]);
+    float od = e.c[k][PO];
+#pragma unroll
+    for (int i = PO - 2; i >= 1; i -= 2) od = fmaf(od, z2, e.c[k][i]);
+    r.w[k] = fmaf(od, z, ev);
+    r.w[W - 1 - k] = fmaf(-od, z, ev);
   }
   return r;
 }
