@@ -456,17 +456,21 @@ def _stage1_extra(args, dev) -> dict:
     res = {}
     vox = torch.tensor(scenes.voxel_grid(128, size=0.32).T.copy(), device=dev)
     target = torch.ones(vox.shape[0], device=dev)
-    for name, prec, mf_prec, graph, iters in (("mixed_graph", "mixed", "mixed", True, 5),
-                                              ("mixed_nufft_mf_graph", "mixed", "nufft", True, 5),
-                                              ("plain_eager", "plain", "plain", False, 1)):
+    for name, prec, mf_prec, bank, graph, iters in (("mixed_graph", "mixed", "mixed", 1, True, 5),
+                                                    ("mixed_nufft_mf_graph", "mixed", "nufft", 1, True, 5),
+                                                    ("mixed_bank2_graph", "mixed", "mixed", 2, True, 5),
+                                                    ("plain_eager", "plain", "plain", 1, False, 1)):
         st = Stage1RFStep(num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=256, voxels=vox,
-                          target_mag=target, precision=prec, device=dev, seed=args.seed, mf_precision=mf_prec)
+                          target_mag=target, precision=prec, device=dev, seed=args.seed, mf_precision=mf_prec,
+                          bank_size=bank)
         if graph:
             st.capture()
         ms = autotune.time_call(st.run, iters=iters, warmup=1)
         res[name] = {"ms": round(ms, 2), "it_per_s": round(1e3 / ms, 2)}
     return {"stage1_step": {"workload": ("128 antennas x 2048 rays x 128 samples, S=256, random-init "
-                                         "SDF MLP, MF onto 128^3 voxels, L1 on |volume|, Adam"),
+                                         "SDF MLP, MF onto 128^3 voxels, L1 on |volume| + eikonal, Adam; "
+                                         "bank2: the reference's 2-chunk antenna bank, one chunk rendered "
+                                         "per step, the bank kept on the GPU"),
                             **res}}
 
 

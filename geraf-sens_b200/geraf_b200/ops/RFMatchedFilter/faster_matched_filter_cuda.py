@@ -18,6 +18,7 @@ import torch
 from torch.autograd import Function
 from torch.autograd.function import once_differentiable
 
+from ...runtime import default_precision
 from . import _C
 
 
@@ -62,7 +63,9 @@ class _FasterMatchedFilterKernel(Function):
         ctx.save_for_backward(_as_contiguous(real_sel), _as_contiguous(image_sel),
                               _as_contiguous(tpos_sel), _as_contiguous(rpos_sel), voxel_soa)
         ctx.sizes = (total_ant_size, num_sel, numADCSample, adcSampleRate, As_sci, N)
-        ctx.precision = precision
+        # the backward runs the form (and NUFFT width) of the forward that ran
+        ctx.precision = precision or default_precision()
+        ctx.taps = (tuning or {}).get("taps")
         return output_real, output_image
 
     @staticmethod
@@ -81,7 +84,7 @@ class _FasterMatchedFilterKernel(Function):
             _C.MatchedFilter_backward_realimag(
                 grad_output_real, grad_output_image, real_sel, image_sel, tpos_sel, rpos_sel,
                 grad_real, grad_image, voxel_soa, num_sel, numADCSample, adcSampleRate, As_sci, N,
-                precision=ctx.precision)
+                precision=ctx.precision, tuning={"taps": ctx.taps} if ctx.taps else None)
             grad_real = grad_real * num_sel / total_ant_size
             grad_image = grad_image * num_sel / total_ant_size
         return (grad_real, grad_image) + (None,) * 15

@@ -19,9 +19,12 @@ Two step shapes that a GeRaF training loop runs:
 
 ``capture()`` records one whole step (forward, backward and, for the stage-1
 step, the optimizer update) into a CUDA graph over static input buffers;
-``run()`` replays it.  All operator calls enqueue on the current stream and
-allocate through PyTorch's caching allocator, which the graph's private pool
-serves during capture.
+``run()`` replays it.  The stage-1 step can also keep the reference's antenna
+bank (``bank_size`` > 1): each step renders one chunk of the antennas and
+matched-filters it with the other chunks' last renders, all in device memory.
+All operator calls enqueue on the current stream and allocate through
+PyTorch's caching allocator, which the graph's private pool serves during
+capture.
 """
 from __future__ import annotations
 
@@ -30,6 +33,7 @@ import math
 import torch
 from torch import nn
 
+from .ops.RFMatchedFilter.faster_matched_filter_cuda import faster_matched_filter_cuda
 from .ops.RFMatchedFilter.matched_filter_cuda import matched_filter_cuda
 from .ops.RFSignalTracer.ragged import signal_tracer_ragged
 from .ops.RFSignalTracer.signal_tracer_cuda import signal_tracer_cuda
@@ -41,12 +45,16 @@ class _Graphable:
     def _step_eager(self) -> torch.Tensor:  # pragma: no cover - abstract
         raise NotImplementedError
 
+    def _advance(self) -> None:
+        """Per-step host-side set-up before a step runs (none by default)."""
+
     def warmup(self, iters: int = 2) -> None:
         """Eager steps on a side stream (autograd and allocator warm-up before capture)."""
         s = torch.cuda.Stream()
         s.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(s):
             for _ in range(iters):
+                self._advance()
                 self._step_eager()
         torch.cuda.current_stream().wait_stream(s)
         torch.cuda.synchronize()
@@ -60,6 +68,7 @@ class _Graphable:
 
     def run(self) -> torch.Tensor:
         """One step: graph replay when captured, else eager."""
+        self._advance()
         if self.graph is not None:
             self.graph.replay()
             return self.static_loss
@@ -103,7 +112,7 @@ class Stage1RFStep(_Graphable):
 
     def __init__(self, num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=128, voxels=None,
                  target_mag=None, precision: str = "mixed", device="cuda", seed=0, lr=5e-4,
-                 mf_precision: str | None = None, grad_regression: float = 0.1):
+                 mf_precision: str | None = None, grad_regression: float = 0.1, bank_size: int = 1):
         from . import scenes
         from .sdf import SDFNetwork
 
@@ -140,6 +149,73 @@ class Stage1RFStep(_Graphable):
         self.voxels = voxels.contiguous()
         self.target = (target_mag if target_mag is not None
                        else torch.ones(self.voxels.shape[0], device=self.device))
+        # Antenna bank (rf_rendering.py:558-604, 682-683, 718-800): the antennas are
+        # split into `bank_size` chunks; a step renders one chunk with gradients and
+        # matched-filters it together with the other chunks' IF from their last
+        # render.  The bank lives in device memory and the chunk's antenna indices in
+        # static index buffers, so a step is one graph replay with no host copies.
+        A = self.tx.shape[0]
+        if bank_size < 1 or A % bank_size:
+            raise ValueError(f"bank_size must divide the {A} antennas, got {bank_size}")
+        self.bank_size = bank_size
+        self.chunk = A // bank_size
+        self._chunk_id = -1
+        if bank_size > 1:
+            self.sel_idx = torch.empty(self.chunk, dtype=torch.int64, device=self.device)
+            self.unsel_idx = torch.empty(A - self.chunk, dtype=torch.int64, device=self.device)
+            S = self.chirp.num_samples
+            self.bank_re = torch.zeros((A, S), device=self.device)
+            self.bank_im = torch.zeros((A, S), device=self.device)
+            self._fill_bank()
+            self._set_chunk(0)   # valid indices from the start; the first step still takes chunk 0
+            self._chunk_id = -1
+
+    def _set_chunk(self, c: int) -> None:
+        """Points the static index buffers at chunk ``c`` (outside any graph)."""
+        A = self.tx.shape[0]
+        ids = torch.arange(A, device=self.device)
+        sel = (ids // self.chunk) == c
+        self.sel_idx.copy_(ids[sel])
+        self.unsel_idx.copy_(ids[~sel])
+        self._chunk_id = c
+
+    def _render_inputs(self, sdf, feat, grad):
+        """Unit normals [P, 3] and amplitudes [1, P] of the ray samples from the SDF."""
+        normals = grad / (grad.norm(dim=-1, keepdim=True) + 1e-12)
+        inv_s = torch.exp(self.log_inv_s)
+        sdf = sdf.reshape(self.R, self.T)
+        cdf = torch.sigmoid(sdf * inv_s)
+        alpha = ((cdf[:, :-1] - cdf[:, 1:]) / (cdf[:, :-1] + 1e-5)).clamp(0.0, 1.0)
+        alpha = torch.cat([alpha, alpha[:, -1:]], 1)
+        # transmittance prod_{j<i} (1 - alpha_j); formed as exp(cumsum(log)) because the
+        # backward of cumprod synchronises with the host, which stream capture forbids
+        log_t = torch.log(1.0 - alpha + 1e-7)
+        trans = torch.exp(torch.cumsum(log_t, 1) - log_t)
+        sig = (alpha * trans * torch.sigmoid(self.head(feat)).reshape(self.R, self.T)).reshape(1, -1)
+        return normals, sig
+
+    def _fill_bank(self) -> None:
+        """Renders every chunk once with the current network (rf_rendering.py:558-604)."""
+        x = ((self.points - self.center) / self.scale).requires_grad_(True)
+        sdf, feat = self.net(x)
+        grad, = torch.autograd.grad(sdf.sum(), x)
+        with torch.no_grad():
+            normals, sig = self._render_inputs(sdf.detach(), feat.detach(), grad)
+            P = self.R * self.T
+            S = self.chirp.num_samples
+            for c in range(self.bank_size):
+                rows = slice(c * self.chunk, (c + 1) * self.chunk)
+                xr, xi = signal_tracer_cuda(normals, sig.expand(self.chunk, P).contiguous(), self.points,
+                                            self.tx[rows].contiguous(), self.rx[rows].contiguous(),
+                                            self.inbounds, S, self.cfg["adcSampleRate"], self.cfg["fc_start"],
+                                            self.cfg["As_sci"], self.chunk, P, precision=self.precision)
+                self.bank_re[rows] = xr
+                self.bank_im[rows] = xi
+
+    def _advance(self) -> None:
+        """With an antenna bank, every step moves on to the next chunk (round-robin)."""
+        if self.bank_size > 1:
+            self._set_chunk((self._chunk_id + 1) % self.bank_size)
 
     def resample(self) -> None:
         """New rays through the scene disk, stratified samples along each (in place)."""
@@ -163,23 +239,30 @@ class Stage1RFStep(_Graphable):
         x = ((self.points - self.center) / self.scale).requires_grad_(True)
         sdf, feat = self.net(x)
         grad, = torch.autograd.grad(sdf.sum(), x, create_graph=True)
-        normals = grad / (grad.norm(dim=-1, keepdim=True) + 1e-12)
-        inv_s = torch.exp(self.log_inv_s)
-        sdf = sdf.reshape(self.R, self.T)
-        cdf = torch.sigmoid(sdf * inv_s)
-        alpha = ((cdf[:, :-1] - cdf[:, 1:]) / (cdf[:, :-1] + 1e-5)).clamp(0.0, 1.0)
-        alpha = torch.cat([alpha, alpha[:, -1:]], 1)
-        # transmittance prod_{j<i} (1 - alpha_j); formed as exp(cumsum(log)) because the
-        # backward of cumprod synchronises with the host, which stream capture forbids
-        log_t = torch.log(1.0 - alpha + 1e-7)
-        trans = torch.exp(torch.cumsum(log_t, 1) - log_t)
-        sig = (alpha * trans * torch.sigmoid(self.head(feat)).reshape(self.R, self.T)).reshape(1, -1)
+        normals, sig = self._render_inputs(sdf, feat, grad)
         P = self.R * self.T
-        xr, xi = signal_tracer_cuda(normals, sig.expand(A, P).contiguous(), self.points, self.tx, self.rx,
-                                    self.inbounds, S, self.cfg["adcSampleRate"], self.cfg["fc_start"],
-                                    self.cfg["As_sci"], A, P, precision=self.precision)
-        yr, yi = matched_filter_cuda(xr, xi, self.tx, self.rx, self.voxels, A, S, self.cfg["adcSampleRate"],
-                                     self.cfg["As_sci"], self.voxels.shape[0], precision=self.mf_precision)
+        N = self.voxels.shape[0]
+        fs, As = self.cfg["adcSampleRate"], self.cfg["As_sci"]
+        if self.bank_size > 1:
+            C = self.chunk
+            tx_s, rx_s = self.tx.index_select(0, self.sel_idx), self.rx.index_select(0, self.sel_idx)
+            tx_u, rx_u = self.tx.index_select(0, self.unsel_idx), self.rx.index_select(0, self.unsel_idx)
+            xr, xi = signal_tracer_cuda(normals, sig.expand(C, P).contiguous(), self.points, tx_s, rx_s,
+                                        self.inbounds, S, fs, self.cfg["fc_start"], As, C, P,
+                                        precision=self.precision)
+            # [rendered chunk; cached chunks], adjoint over the rendered chunk only
+            yr, yi = faster_matched_filter_cuda(xr, xi, self.bank_re.index_select(0, self.unsel_idx),
+                                                self.bank_im.index_select(0, self.unsel_idx), tx_s, rx_s,
+                                                tx_u, rx_u, self.voxels, A, C, S, fs, As, N,
+                                                precision=self.mf_precision)
+            self.bank_re.index_copy_(0, self.sel_idx, xr.detach())
+            self.bank_im.index_copy_(0, self.sel_idx, xi.detach())
+        else:
+            xr, xi = signal_tracer_cuda(normals, sig.expand(A, P).contiguous(), self.points, self.tx, self.rx,
+                                        self.inbounds, S, fs, self.cfg["fc_start"], As, A, P,
+                                        precision=self.precision)
+            yr, yi = matched_filter_cuda(xr, xi, self.tx, self.rx, self.voxels, A, S, fs, As, N,
+                                         precision=self.mf_precision)
         mag = torch.sqrt(yr * yr + yi * yi + 1e-20)
         loss = (mag / (mag.detach().mean() + 1e-20) - self.target).abs().mean()
         if self.grad_regression:

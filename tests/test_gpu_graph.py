@@ -63,3 +63,25 @@ def test_stage1_step_graph_matches_eager_and_trains(cuda, precision):
     assert loss3 == pytest.approx(losses[2], rel=1e-5)
     more = [graphed.run().item() for _ in range(5)]
     assert np.isfinite(more).all() and more[-1] != more[0]
+
+
+def test_stage1_antenna_bank_matches_full_step_and_replays(cuda):
+    """With the network unchanged, the banked step's first loss equals the full
+    step's (the bank holds every chunk rendered by the same network); the banked
+    step rotates through its chunks identically eager and graph-replayed."""
+    from geraf_b200.step import Stage1RFStep
+
+    kw = dict(num_antennas=8, num_rays=128, samples_per_ray=32, num_adc=32, precision="mixed", seed=5)
+    full = Stage1RFStep(**kw).run().item()
+    banked = Stage1RFStep(bank_size=4, **kw)
+    assert banked.run().item() == pytest.approx(full, rel=1e-5)
+
+    eager = Stage1RFStep(bank_size=2, **kw)
+    losses = [eager.run().item() for _ in range(4)]
+    graphed = Stage1RFStep(bank_size=2, **kw)
+    graphed.capture()          # two eager warm-up steps (chunks 0, 1), then records a step
+    more = [graphed.run().item() for _ in range(2)]   # replays on chunks 0, 1
+    torch.cuda.synchronize()
+    assert np.isfinite(losses).all() and np.isfinite(more).all()
+    assert more[0] == pytest.approx(losses[2], rel=1e-5)
+    assert more[1] == pytest.approx(losses[3], rel=1e-5)
