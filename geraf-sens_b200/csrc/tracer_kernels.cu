@@ -912,7 +912,10 @@ BiP<T> make_bi(const BilinearArgs& a) {
 // ---------------------------------------------------------------------------
 Tuning tracer_forward_resolve(const TracerArgs& a, const Tuning& req) {
   Tuning t = req;
-  if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 256;
+  // MIXED: 64-thread blocks (measured on B200 for 64 antennas x 524288 points x 128
+  // samples: 0.66 ms against 0.84 ms with 256 threads -- the per-tile compaction
+  // barriers stall fewer warps, and more blocks fit each SM).
+  if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = a.mode == kMixed ? 64 : 256;
   if (t.chunk != 8 && t.chunk != 16 && t.chunk != 32) t.chunk = 16;
   if (t.items <= 0) t.items = 1;
   if (t.stage_rows <= 0) t.stage_rows = 8;
