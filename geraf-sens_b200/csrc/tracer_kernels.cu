@@ -54,6 +54,7 @@ struct TrP {
   int groups;         // forward: sample groups per block
   int rows, ld, bulk;  // adjoint: antenna stage
   size_t pos_off, buf_off;
+  size_t cnt_off, list_off, contrib_off;  // MIXED adjoint: per-tile work lists
 };
 
 template <typename T>
@@ -289,6 +290,30 @@ AdjSmem adj_smem_layout(int rows, int ld) {
   return s;
 }
 
+// MIXED adjoint: the staged ring as above, then per-tile work lists -- live
+// (point, antenna) counts [rows], their point slots [rows][threads] and the
+// per-point gradient contributions [rows][nc][threads].
+struct AdjMixedSmem {
+  size_t pos_off, buf_off, cnt_off, list_off, contrib_off, total;
+};
+
+template <typename T>
+AdjMixedSmem adj_mixed_smem_layout(int rows, int ld, int threads, int nc) {
+  const AdjSmem base = adj_smem_layout<T>(rows, ld);
+  AdjMixedSmem s;
+  s.pos_off = base.pos_off;
+  s.buf_off = base.buf_off;
+  size_t off = base.total;
+  s.cnt_off = off;
+  off += (static_cast<size_t>(rows) * sizeof(int) + 127) & ~static_cast<size_t>(127);
+  s.list_off = off;
+  off += (static_cast<size_t>(rows) * threads * sizeof(int) + 127) & ~static_cast<size_t>(127);
+  s.contrib_off = off;
+  off += static_cast<size_t>(rows) * nc * threads * sizeof(float);
+  s.total = (off + 127) & ~static_cast<size_t>(127);
+  return s;
+}
+
 template <typename T>
 __device__ __forceinline__ void stage_positions_f(float* pos, int stage, int rows_max, const T* tx,
                                                   const T* rx, int64_t a0, int rws) {
@@ -447,20 +472,34 @@ __global__ void __launch_bounds__(128) tracer_bwd_plain_kernel(const TrP<T> p) {
   if (inside) store_point_grads(p, split, pi, accum_grad_normal, accum_grad_point, WITH_POINTS);
 }
 
-// MIXED adjoint: thread = VPT points; per (point, antenna) the residual
-// polynomial Q(zeta) = sum_n conj(g[a,n]) zeta^n is evaluated by Horner
-// (4 FMA per sample) and, for position gradients, Q1 = sum_n n conj(g) zeta^n
-// alongside (4 more FMA per sample).
+// MIXED adjoint: a block owns blockDim points (one per thread) and streams
+// antenna rows of the residual through a TMA ring.  Per (point, antenna) the
+// residual polynomial Q(zeta) = sum_n conj(g[a,n]) zeta^n is evaluated by
+// Horner (4 FMA per sample) and, for position gradients, Q1 = sum_n n conj(g)
+// zeta^n alongside (4 more FMA per sample).
+//
+// Culled pairs (back-facing or grazing, rho < 1e-6) skip all of that, so per
+// stage the block first lists its live (point, antenna) pairs and then deals
+// them out evenly over all threads: no lane idles beside a lane that works.
+// Each pair's normal / position contributions land in shared memory, and the
+// point's owner thread adds them up in antenna order -- the same sums, in the
+// same order, as one thread walking its point's antennas.
 template <typename T, bool WITH_POINTS>
 __global__ void __launch_bounds__(128) tracer_bwd_mixed_kernel(const TrP<T> p) {
+  constexpr int NC = WITH_POINTS ? 6 : 3;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
   float* pos = reinterpret_cast<float*>(smem + p.pos_off);
+  int* cnt = reinterpret_cast<int*>(smem + p.cnt_off);           // [rows]
+  int* list = reinterpret_cast<int*>(smem + p.list_off);         // [rows][TILE]
+  float* contrib = reinterpret_cast<float*>(smem + p.contrib_off);  // [rows][NC][TILE]
   PairStager<T> stg{reinterpret_cast<T*>(smem + p.buf_off), bar, p.ld, p.rows, p.bulk != 0};
 
+  const int TILE = blockDim.x;
   const int split = blockIdx.x % p.splits;
   const int64_t ptile = blockIdx.x / p.splits;
-  const int64_t pi = ptile * blockDim.x + threadIdx.x;
+  const int64_t p_base = ptile * TILE;
+  const int64_t pi = p_base + threadIdx.x;
   const int64_t a_begin = static_cast<int64_t>(split) * p.per_split;
   const int64_t a_end = min(p.A, a_begin + p.per_split);
   const int ntiles = a_end > a_begin ? ceil_div(a_end - a_begin, p.rows) : 0;
@@ -474,12 +513,11 @@ __global__ void __launch_bounds__(128) tracer_bwd_mixed_kernel(const TrP<T> p) {
   }
   __syncthreads();
 
-  float nrm[3] = {0.0f, 0.0f, 1.0f}, pt[3] = {0.0f, 0.0f, 0.0f};
+  float own_nrm[3] = {0.0f, 0.0f, 1.0f}, own_pt[3] = {0.0f, 0.0f, 0.0f};
   if (active) {
-    load3(p.normals, pi, nrm);
-    load3(p.points, pi, pt);
+    load3(p.normals, pi, own_nrm);
+    load3(p.points, pi, own_pt);
   }
-  const double px = pt[0], py = pt[1], pz = pt[2];
   // w0 and w1/fs in rad per unit delay, as exact FP64 products of the FP32 constants.
   const float w0 = static_cast<float>(2.0 * static_cast<double>(kPiF) * p.f0);
   const float w1s = static_cast<float>(2.0 * static_cast<double>(kPiF) * p.As / p.fs);
@@ -497,27 +535,58 @@ __global__ void __launch_bounds__(128) tracer_bwd_mixed_kernel(const TrP<T> p) {
 
   for (int t = 0; t < ntiles; ++t) {
     const int s = t & 1;
-    if (!stg.wait(s, (t >> 1) & 1, p.status)) {
+    for (int r = threadIdx.x; r < p.rows; r += TILE) cnt[r] = 0;
+    if (!stg.wait(s, (t >> 1) & 1, p.status)) {  // (its barrier also publishes cnt)
       if (t + 1 < ntiles) stg.drain(s ^ 1, ((t + 1) >> 1) & 1, p.status);
       return;
     }
     const int64_t a0 = a_begin + static_cast<int64_t>(t) * p.rows;
     const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
-    for (int r = 0; r < rws && inside; ++r) {
+
+    // 1. list the live pairs of the stage; dead pairs get zero gradients
+    for (int r = 0; r < rws; ++r) {
+      if (!inside) break;
+      const float* ps = pos + (s * p.rows + r) * 6;
+      const float txp[3] = {ps[0], ps[1], ps[2]};
+      const float rxp[3] = {ps[3], ps[4], ps[5]};
+      bool live = false;
+      if (active) {
+        SpecGeom geo;
+        specular_geometry(txp, rxp, own_nrm, own_pt, geo);
+        live = !culled(geo);
+      }
+      if (live) {
+        list[r * TILE + atomicAdd(&cnt[r], 1)] = threadIdx.x;
+      } else {
+        p.g_sigmas[(a0 + r) * p.P + pi] = from_f<T>(0.0f);
+#pragma unroll
+        for (int k = 0; k < NC; ++k) contrib[(r * NC + k) * TILE + threadIdx.x] = 0.0f;
+      }
+    }
+    __syncthreads();
+
+    // 2. every thread takes live pairs k = tid, tid + TILE, ... in (row, list) order
+    int total = 0;
+    for (int r = 0; r < rws; ++r) total += cnt[r];
+    int r_cur = 0, r_start = 0;
+    for (int k = threadIdx.x; k < total; k += TILE) {
+      while (k >= r_start + cnt[r_cur]) {
+        r_start += cnt[r_cur];
+        ++r_cur;
+      }
+      const int r = r_cur;
+      const int slot = list[r * TILE + (k - r_start)];
+      const int64_t pj = p_base + slot;
       const int64_t a = a0 + r;
+      float nrm[3], pt[3];
+      load3(p.normals, pj, nrm);
+      load3(p.points, pj, pt);
       const float* ps = pos + (s * p.rows + r) * 6;
       const float txp[3] = {ps[0], ps[1], ps[2]};
       const float rxp[3] = {ps[3], ps[4], ps[5]};
       SpecGeom geo;
-      bool live = false;
-      if (active) {
-        specular_geometry(txp, rxp, nrm, pt, geo);
-        live = !culled(geo);
-      }
-      if (!live) {
-        p.g_sigmas[a * p.P + pi] = from_f<T>(0.0f);
-        continue;
-      }
+      specular_geometry(txp, rxp, nrm, pt, geo);
+      const double px = pt[0], py = pt[1], pz = pt[2];
       const PhaseCycles pc = path_cycles(ps[0] - px, ps[1] - py, ps[2] - pz, ps[3] - px,
                                          ps[4] - py, ps[5] - pz, p.k0, p.b0, p.k1, p.b1);
       const float2 zt = cis_cycles(pc.dcyc);
@@ -551,14 +620,14 @@ __global__ void __launch_bounds__(128) tracer_bwd_mixed_kernel(const TrP<T> p) {
       const float sum_re = eq.x;
       const float propagation_distance = path_distance(txp, rxp, pt);
       const float propagation_attenuation = 1.0f / sq(propagation_distance);
-      const float sigma_value = ld_f(p.sigmas, a * p.P + pi);
-      p.g_sigmas[a * p.P + pi] =
+      const float sigma_value = ld_f(p.sigmas, a * p.P + pj);
+      p.g_sigmas[a * p.P + pj] =
           from_f<T>(propagation_attenuation * geo.align * sum_re / static_cast<float>(p.P));
       float gsa[3];
       align_normal_gradient(geo, nrm, gsa);
       const float normal_scale = sigma_value * propagation_attenuation;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) gnorm[k] += normal_scale * gsa[k] * sum_re;
+      for (int c = 0; c < 3; ++c) contrib[(r * NC + c) * TILE + slot] = normal_scale * gsa[c] * sum_re;
       if (WITH_POINTS) {
         // Q1 = zeta Q'(zeta);  sum_n w_n (g_i cos - g_r sin) = -Im(exp(j phi0) (w0 Q + w1s Q1))
         const float2 q1 = cmul(zt, make_float2(dr, di));
@@ -570,11 +639,24 @@ __global__ void __launch_bounds__(128) tracer_bwd_mixed_kernel(const TrP<T> p) {
         float drho[3];
         align_point_gradient(geo, nrm, dist_t, dist_r, drho);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const float dD = geo.inc[k] - geo.ret[k];
+        for (int c = 0; c < 3; ++c) {
+          const float dD = geo.inc[c] - geo.ret[c];
           const float damp_dp =
-              normal_scale * drho[k] - 2.0f * amp / propagation_distance * dD;
-          gpt[k] += sum_re * damp_dp + d_tau * dD / kSpeedOfLight;
+              normal_scale * drho[c] - 2.0f * amp / propagation_distance * dD;
+          contrib[(r * NC + 3 + c) * TILE + slot] = sum_re * damp_dp + d_tau * dD / kSpeedOfLight;
+        }
+      }
+    }
+    __syncthreads();
+
+    // 3. each owner adds its point's contributions in antenna order
+    if (inside) {
+      for (int r = 0; r < rws; ++r) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) gnorm[c] += contrib[(r * NC + c) * TILE + threadIdx.x];
+        if (WITH_POINTS) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) gpt[c] += contrib[(r * NC + 3 + c) * TILE + threadIdx.x];
         }
       }
     }
@@ -851,11 +933,20 @@ cudaError_t launch_tracer_bwd(const TracerArgs& a, const Tuning& t, void* ws, cu
                ? 1
                : 0;
   int rows = t.stage_rows;
-  AdjSmem lay = adj_smem_layout<T>(rows, p.ld);
+  const bool with_points = a.grad_points != nullptr;
+  const int nc = with_points ? 6 : 3;
+  auto layout = [&](int rw) {
+    if (a.mode == kPlain) {
+      const AdjSmem b = adj_smem_layout<T>(rw, p.ld);
+      return AdjMixedSmem{b.pos_off, b.buf_off, 0, 0, 0, b.total};
+    }
+    return adj_mixed_smem_layout<T>(rw, p.ld, threads, nc);
+  };
+  AdjMixedSmem lay = layout(rows);
   const DeviceInfo dev = current_device_info();
   while (rows > 1 && lay.total > static_cast<size_t>(dev.max_smem_optin)) {
     rows /= 2;
-    lay = adj_smem_layout<T>(rows, p.ld);
+    lay = layout(rows);
   }
   if (rows != t.stage_rows) {
     p.per_split = ((std::max<int64_t>(1, (a.A + rows - 1) / rows) + t.splits - 1) / t.splits) * rows;
@@ -863,7 +954,9 @@ cudaError_t launch_tracer_bwd(const TracerArgs& a, const Tuning& t, void* ws, cu
   p.rows = rows;
   p.pos_off = lay.pos_off;
   p.buf_off = lay.buf_off;
-  const bool with_points = a.grad_points != nullptr;
+  p.cnt_off = lay.cnt_off;
+  p.list_off = lay.list_off;
+  p.contrib_off = lay.contrib_off;
   const void* fn;
   if (a.mode == kPlain) {
     fn = with_points ? reinterpret_cast<const void*>(&tracer_bwd_plain_kernel<T, true>)
