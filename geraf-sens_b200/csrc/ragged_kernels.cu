@@ -165,19 +165,27 @@ __global__ void __launch_bounds__(256) ragged_fwd_kernel(const RgP<T> p) {
 #pragma unroll
     for (int m = 0; m < K; ++m) accr[m] = acci[m] = hir[m] = hii[m] = 0.0f;
 
+    // The point data of tile k + 1 are loaded while tile k's samples are summed.
+    float nrm[3] = {0.0f, 0.0f, 1.0f}, pt[3] = {0.0f, 0.0f, 0.0f}, sig = 0.0f;
+    bool inb = false;
+    auto load_point = [&](int64_t q) {
+      inb = q < pt_end && (p.inb == nullptr || p.inb[q]);
+      if (inb) {
+        ld3(p.normals, q, nrm);
+        ld3(p.points, q, pt);
+        sig = ld_f(p.sigmas, q);
+      }
+    };
+    load_point(pt_begin + threadIdx.x);
     for (int64_t p0 = pt_begin; p0 < pt_end; p0 += TILE) {
-      const int64_t pi = p0 + threadIdx.x;
       bool valid = false;
       float2 w = make_float2(0.0f, 0.0f), zt = make_float2(1.0f, 0.0f), zk = make_float2(1.0f, 0.0f);
-      if (pi < pt_end && (p.inb == nullptr || p.inb[pi])) {
-        float nrm[3], pt[3];
-        ld3(p.normals, pi, nrm);
-        ld3(p.points, pi, pt);
+      if (inb) {
         SpecGeom geo;
         specular_geometry(txp, rxp, nrm, pt, geo);
         if (!culled(geo)) {
           const float propagation_distance = path_distance(txp, rxp, pt);
-          const float amp = ld_f(p.sigmas, pi) * geo.align / sq(propagation_distance);
+          const float amp = sig * geo.align / sq(propagation_distance);
           const double px = pt[0], py = pt[1], pz = pt[2];
           const PhaseCycles pc = path_cycles(tx - px, ty - py, tz - pz, rx - px, ry - py, rz - pz,
                                              p.k0, p.b0, p.k1, p.b1);
@@ -211,6 +219,7 @@ __global__ void __launch_bounds__(256) ragged_fwd_kernel(const RgP<T> p) {
           w = cmul(w, zk);
         }
       }
+      load_point(p0 + TILE + threadIdx.x);  // in flight during the sums below
       __syncthreads();
       for (int vl = l; vl < count; vl += L) {
         float2 s = seeds[g * TILE + vl];
