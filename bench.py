@@ -458,6 +458,7 @@ def _stage1_extra(args, dev) -> dict:
     target = torch.ones(vox.shape[0], device=dev)
     for name, prec, mf_prec, bank, graph, iters in (("mixed_graph", "mixed", "mixed", 1, True, 5),
                                                     ("mixed_nufft_mf_graph", "mixed", "nufft", 1, True, 5),
+                                                    ("nufft_graph", "nufft", "nufft", 1, True, 5),
                                                     ("mixed_bank2_graph", "mixed", "mixed", 2, True, 5),
                                                     ("plain_eager", "plain", "plain", 1, False, 1)):
         st = Stage1RFStep(num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=256, voxels=vox,
@@ -579,7 +580,8 @@ def _tracer_extra(args, dev) -> dict:
     gs = torch.empty((At, P), device=dev)
     gp = torch.empty((P, 3), device=dev)
     tr = {}
-    for prec in ("mixed", "plain"):
+    outs = {}
+    for prec in ("mixed", "nufft", "plain"):
         def step(prec=prec):
             trc.SignalTracer_forward(tw["normals"], tw["sigmas"], tw["points"], tw["tx"], tw["rx"],
                                      tw["inbounds"], xr, xi, St, cfg["adcSampleRate"], cfg["fc_start"],
@@ -587,14 +589,22 @@ def _tracer_extra(args, dev) -> dict:
             trc.SignalTracer_backward_normal_sigma(gxr, gxi, tw["normals"], tw["sigmas"], tw["points"],
                                                    tw["tx"], tw["rx"], tw["inbounds"], gn, gs, St,
                                                    cfg["adcSampleRate"], cfg["fc_start"], cfg["As_sci"],
-                                                   At, P, grad_points=gp if prec == "mixed" else None,
+                                                   At, P, grad_points=gp if prec != "plain" else None,
                                                    precision=prec)
-        ms = autotune.time_call(step, iters=3 if prec == "mixed" else 1, warmup=1)
+        ms = autotune.time_call(step, iters=3 if prec != "plain" else 1, warmup=1)
         tr[prec] = {"rays_per_s": round(At * tw["rays"] / (ms * 1e-3), 1), "ms": round(ms, 3),
                     "gpts_per_s": round(float(At) * P * St / (ms * 1e-3) / 1e9, 2)}
+        outs[prec] = [torch.complex(xr, xi).to(torch.complex128)] + [t.double().clone() for t in (gs, gn, gp)]
+
+    def rel(a, b):
+        return float((a - b).norm() / b.norm())
+
+    tr["nufft"]["rel_l2_vs_mixed"] = {k: rel(outs["nufft"][i], outs["mixed"][i])
+                                      for i, k in enumerate(("signal", "grad_sigmas", "grad_normals",
+                                                             "grad_points"))}
     res["tracer"] = {"workload": f"{At} antennas x {tw['rays']} rays x {P // tw['rays']} samples, S={St}",
                      "unit": "rays/s (ray = ray x antenna pair)", "mixed_with_point_grads": tr["mixed"],
-                     "plain": tr["plain"]}
+                     "nufft_with_point_grads": tr["nufft"], "plain": tr["plain"]}
     return res
 
 

@@ -132,7 +132,11 @@ int32_t check_tracer_sizes(int64_t A, int64_t S, int64_t P, int32_t dtype, int32
     return fail(GERAF_ERR_INVALID_ARGUMENT,
                 std::string("\"signal_tracer\" not implemented for '") + dtype_name(dtype) + "'");
   }
-  REQUIRE(mode == GERAF_MODE_PLAIN || mode == GERAF_MODE_MIXED, "mode must be PLAIN or MIXED");
+  REQUIRE(mode == GERAF_MODE_PLAIN || mode == GERAF_MODE_MIXED || mode == GERAF_MODE_NUFFT,
+          "mode must be PLAIN, MIXED or NUFFT");
+  if (mode == GERAF_MODE_NUFFT && !mf_nufft_supported(S)) {
+    return fail(GERAF_ERR_UNSUPPORTED, "NUFFT signal tracer needs num_adc_samples <= 4096");
+  }
   return GERAF_OK;
 }
 

@@ -120,6 +120,20 @@ Tuning tracer_backward_resolve(const TracerArgs& a, const Tuning& req);
 size_t tracer_backward_workspace(const TracerArgs& a, const Tuning& t);
 cudaError_t tracer_backward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st);
 
+// Fast approximate tracer (MODE_NUFFT, nufft_tracer_kernels.cu); the generic
+// tracer_* entry points dispatch here for that mode.
+Tuning tracer_nufft_forward_resolve(const TracerArgs& a, const Tuning& req);
+size_t tracer_nufft_forward_workspace(const TracerArgs& a, const Tuning& t);
+cudaError_t tracer_nufft_forward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st);
+Tuning tracer_nufft_backward_resolve(const TracerArgs& a, const Tuning& req);
+size_t tracer_nufft_backward_workspace(const TracerArgs& a, const Tuning& t);
+cudaError_t tracer_nufft_backward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st);
+
+// Sums `splits` [P][6] partial point gradients in split order and divides by P
+// into grad_normals (and grad_points when non-null).
+cudaError_t launch_tracer_bwd_finalize(int dtype, const float* partial, int splits, int64_t P, void* g_normals,
+                                       void* g_points, cudaStream_t st);
+
 // Batched tracer over antennas with uneven point sets (CSR point_offsets [A+1]).
 struct RaggedArgs {
   const void* normals;      // [P,3]

@@ -1012,7 +1012,21 @@ BiP<T> make_bi(const BilinearArgs& a) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+cudaError_t launch_tracer_bwd_finalize(int dtype, const float* partial, int splits, int64_t P, void* g_normals,
+                                       void* g_points, cudaStream_t st) {
+  const int blocks = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((P + 255) / 256, 148 * 16)));
+  if (dtype == kF64) {
+    tracer_bwd_finalize_kernel<double><<<blocks, 256, 0, st>>>(partial, splits, P, static_cast<double*>(g_normals),
+                                                               static_cast<double*>(g_points));
+  } else {
+    tracer_bwd_finalize_kernel<float><<<blocks, 256, 0, st>>>(partial, splits, P, static_cast<float*>(g_normals),
+                                                              static_cast<float*>(g_points));
+  }
+  return cudaGetLastError();
+}
+
 Tuning tracer_forward_resolve(const TracerArgs& a, const Tuning& req) {
+  if (a.mode == kNufft) return tracer_nufft_forward_resolve(a, req);
   Tuning t = req;
   // MIXED: 64-thread blocks (measured on B200 for 64 antennas x 524288 points x 128
   // samples: 0.66 ms against 0.84 ms with 256 threads -- the per-tile compaction
@@ -1039,17 +1053,20 @@ Tuning tracer_forward_resolve(const TracerArgs& a, const Tuning& req) {
 }
 
 size_t tracer_forward_workspace(const TracerArgs& a, const Tuning& t) {
+  if (a.mode == kNufft) return tracer_nufft_forward_workspace(a, t);
   if (a.mode == kPlain || t.splits <= 1) return 0;
   return static_cast<size_t>(t.splits) * a.A * a.S * 2 * sizeof(float);
 }
 
 cudaError_t tracer_forward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  if (a.mode == kNufft) return tracer_nufft_forward(a, t, ws, st);
   if (a.A == 0 || a.S == 0) return cudaSuccess;
   if (a.dtype == kF64) return launch_tracer_fwd<double>(a, t, ws, st);
   return launch_tracer_fwd<float>(a, t, ws, st);
 }
 
 Tuning tracer_backward_resolve(const TracerArgs& a, const Tuning& req) {
+  if (a.mode == kNufft) return tracer_nufft_backward_resolve(a, req);
   Tuning t = req;
   if (t.threads != 64 && t.threads != 128) t.threads = 128;
   if (t.items <= 0) t.items = 1;
@@ -1068,11 +1085,13 @@ Tuning tracer_backward_resolve(const TracerArgs& a, const Tuning& req) {
 }
 
 size_t tracer_backward_workspace(const TracerArgs& a, const Tuning& t) {
+  if (a.mode == kNufft) return tracer_nufft_backward_workspace(a, t);
   if (t.splits <= 1 || a.P == 0) return 0;
   return static_cast<size_t>(t.splits) * a.P * 6 * sizeof(float);
 }
 
 cudaError_t tracer_backward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  if (a.mode == kNufft) return tracer_nufft_backward(a, t, ws, st);
   if (a.P == 0) return cudaSuccess;
   if (a.dtype == kF64) return launch_tracer_bwd<double>(a, t, ws, st);
   return launch_tracer_bwd<float>(a, t, ws, st);

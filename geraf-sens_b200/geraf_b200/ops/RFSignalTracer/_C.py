@@ -70,7 +70,7 @@ def SignalTracer_forward(normals, sigmas, points, tx_pos, rx_pos, inbounds, outp
     _check_tracer(normals, sigmas, points, tx_pos, rx_pos, inbounds, output_real, output_imag,
                   S, A, P)
     dt = dtype_code(normals, "signal_tracer_forward_cuda", allow_half=False)
-    mode = mode_code(precision)
+    mode = mode_code(precision, allow_nufft=True)
     tun = tuning_struct("tracer_forward", (A, S, P), mode, tuning)
     with device_guard(normals.device):
         nbytes = _lib.workspace_bytes("geraf_tracer_forward_workspace_bytes", A, S, P, dt, mode,
@@ -107,7 +107,7 @@ def SignalTracer_backward_normal_sigma(grad_output_real, grad_output_imag, norma
                     "`grad_points` must have shape [P, 3].")
         check_same_dtype(normals, (grad_points, "grad_points"))
     dt = dtype_code(grad_output_real, "signal_tracer_backward_normal_sigma_cuda", allow_half=False)
-    mode = mode_code(precision)
+    mode = mode_code(precision, allow_nufft=True)
     tun = tuning_struct("tracer_backward", (A, S, P), mode, tuning)
     with device_guard(grad_output_real.device):
         nbytes = _lib.workspace_bytes("geraf_tracer_backward_workspace_bytes", A, S, P, dt, mode,

@@ -15,6 +15,7 @@ import torch
 from torch.autograd import Function
 from torch.autograd.function import once_differentiable
 
+from ...runtime import default_precision
 from . import _C
 
 
@@ -61,7 +62,9 @@ class _SignalTracerFunction(Function):
         ctx.scalars = (numADCSample, adcSampleRate, fc_start, As_sci, total_ant_size,
                        total_point_size)
         ctx.nomralization = nomralization
-        ctx.precision = precision
+        # the backward runs the form (and NUFFT width) of the forward that ran
+        ctx.precision = precision or default_precision()
+        ctx.taps = (tuning or {}).get("taps")
         return output_real, output_imag
 
     @staticmethod
@@ -81,7 +84,8 @@ class _SignalTracerFunction(Function):
             _C.SignalTracer_backward_normal_sigma(
                 grad_output_real, grad_output_imag, normals, sigmas, points, antenna_t, antenna_r,
                 inbounds, full_grad_normals, full_grad_sigmas, numADCSample, adcSampleRate,
-                fc_start, As_sci, A, P, grad_points=full_grad_points, precision=ctx.precision)
+                fc_start, As_sci, A, P, grad_points=full_grad_points, precision=ctx.precision,
+                tuning={"taps": ctx.taps} if ctx.taps else None)
             grad_normals = full_grad_normals if want_n else None
             grad_sigmas = full_grad_sigmas if want_s else None
             grad_points = full_grad_points

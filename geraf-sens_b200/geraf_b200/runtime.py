@@ -36,10 +36,10 @@ def default_precision() -> str:
     ``mixed`` (FP64 phase reduction, Horner / rotator phasors, compensated
     sums; judged against an FP64 oracle) unless ``GERAF_RF_PRECISION`` names
     ``plain`` (the reference's FP32 arithmetic, expression for expression) or
-    ``nufft`` (the matched filter's fast approximate form: MIXED phases, the
-    sample sum through an oversampled range FFT and a short interpolation
-    kernel; other operators run ``mixed`` under it), or a :func:`precision`
-    context is active.
+    ``nufft`` (the fast approximate form of the matched filter and the signal
+    tracer: MIXED phases, the sample sums through oversampled range FFTs and a
+    short interpolation kernel; operators without it run ``mixed`` under it),
+    or a :func:`precision` context is active.
     """
     override = getattr(_state, "precision", None)
     if override is not None:
@@ -63,14 +63,14 @@ def precision(mode: str):
 
 def mode_code(precision_: str | None, allow_nufft: bool = False) -> int:
     """C-ABI arithmetic form of a call.  ``nufft`` exists for the matched
-    filter only: named explicitly elsewhere it is an error, as the ambient
-    default it means ``mixed``."""
+    filter and the signal tracer: named explicitly for another operator it is
+    an error, as the ambient default it means ``mixed`` there."""
     p = precision_ or default_precision()
     if p not in PRECISIONS:
         raise ValueError(f"precision must be one of {PRECISIONS}, got {p!r}")
     if p == "nufft" and not allow_nufft:
         if precision_ is not None:
-            raise ValueError("precision 'nufft' is only available for the matched filter")
+            raise ValueError("precision 'nufft' is only available for the matched filter and the signal tracer")
         p = "mixed"
     return _MODES[p]
 

@@ -60,14 +60,14 @@ extern "C" {
  *        (relative L2 <= 1e-4).                                              */
 #define GERAF_MODE_PLAIN 0
 #define GERAF_MODE_MIXED 1
-/* NUFFT (matched filter only; no reference counterpart): the MIXED phase
- *        model with the per-antenna sample sum evaluated through an
- *        oversampled range FFT of each antenna's samples and a W-point
- *        "exponential of semicircle" interpolation kernel, O(W) instead of
- *        O(S) work per (voxel, antenna).  A fast approximate form: relative
- *        L2 against the FP64 oracle ~1e-6 at W = 8 (tuning.taps), ~1e-3 at
- *        W = 4.  Needs num_adc_samples <= 4096.  The adjoint is the exact
- *        adjoint of this forward.                                          */
+/* NUFFT (matched filter and signal tracer; no reference counterpart): the
+ *        MIXED phase model with the per-antenna sample sums evaluated through
+ *        oversampled range FFTs and a W-point "exponential of semicircle"
+ *        interpolation kernel, O(W) instead of O(S) work per
+ *        (voxel|point, antenna).  A fast approximate form: relative L2
+ *        against the FP64 oracle ~1e-6 at W = 8 (tuning.taps), ~1e-3 at
+ *        W = 4.  Needs num_adc_samples <= 4096.  Each adjoint is the exact
+ *        adjoint of its forward.  Not available for the ragged tracer.     */
 #define GERAF_MODE_NUFFT 2
 
 /* Launch shape.  Any field left 0 takes the library default for the call. */

@@ -205,8 +205,9 @@ def test_argument_checks(cuda, case):
     out = torch.empty(8, device="cuda")
     with pytest.raises(RuntimeError, match="4096"):
         _C.MatchedFilter_forward(z, z, pos, pos, out, out.clone(), vox, A, S, 5e6, 1e6, 8, precision="nufft")
-    with pytest.raises(ValueError, match="matched filter"):
+    xr = torch.empty((A, S), device="cuda")
+    with pytest.raises(RuntimeError, match="4096"):
         _T.SignalTracer_forward(torch.zeros((8, 3), device="cuda"), torch.zeros((A, 8), device="cuda"),
                                 torch.zeros((8, 3), device="cuda"), pos, pos,
-                                torch.ones(8, dtype=torch.bool, device="cuda"), z[:, :16].contiguous(),
-                                z[:, :16].contiguous(), 16, 5e6, 770.0, 1e6, A, 8, precision="nufft")
+                                torch.ones(8, dtype=torch.bool, device="cuda"), xr, xr.clone(), S, 5e6,
+                                770.0, 1e6, A, 8, precision="nufft")
