@@ -9,9 +9,9 @@ Two step shapes that a GeRaF training loop runs:
   filter adjoint and the tracer adjoint onto the points' amplitudes, normals
   and positions.
 * :class:`Stage1RFStep` -- a GeRaF stage-1 RF step on synthetic data: a
-  random-init NeuS SDF MLP evaluated on ray samples gives normals (SDF
-  gradient, differentiable) and amplitudes (alpha-composited weights x
-  reflectance); the tracer renders the IF of a bank of antennas from the shared
+  random-init NeuS SDF MLP evaluated on ray samples (under FP16 autocast, as
+  the reference) gives normals (SDF gradient, differentiable) and amplitudes
+  (alpha-composited weights x reflectance); the tracer renders the IF of a bank of antennas from the shared
   points, the matched filter images it onto target voxels, an L1 loss on the
   magnitude against a target volume, plus the eikonal regulariser on the SDF
   gradient, is back-propagated (double backward through the SDF gradient) and
@@ -112,7 +112,8 @@ class Stage1RFStep(_Graphable):
 
     def __init__(self, num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=128, voxels=None,
                  target_mag=None, precision: str = "mixed", device="cuda", seed=0, lr=5e-4,
-                 mf_precision: str | None = None, grad_regression: float = 0.1, bank_size: int = 1):
+                 mf_precision: str | None = None, grad_regression: float = 0.1, bank_size: int = 1,
+                 sdf_fp16: bool = True):
         from . import scenes
         from .sdf import SDFNetwork
 
@@ -124,6 +125,9 @@ class Stage1RFStep(_Graphable):
         # eikonal regulariser weight (the reference's `with_grad_regression`, 0.1 in
         # configs/geraf/bunnyboxv1/geraf2_bunnyboxv1_stage1.py:62)
         self.grad_regression = grad_regression
+        # the SDF network and its gradient run under FP16 autocast, as the reference's
+        # stage-1 loss does (rf_rendering.py:742-749); the RF operators get FP32
+        self.sdf_fp16 = sdf_fp16
         self.net = SDFNetwork().to(self.device)
         self.head = nn.Linear(256, 1).to(self.device)
         self.log_inv_s = nn.Parameter(torch.tensor(10 * 0.3, device=self.device))  # inv_s = e^3
@@ -194,11 +198,17 @@ class Stage1RFStep(_Graphable):
         sig = (alpha * trans * torch.sigmoid(self.head(feat)).reshape(self.R, self.T)).reshape(1, -1)
         return normals, sig
 
+    def _sdf(self, x, create_graph: bool):
+        """SDF, feature vector and SDF gradient at normalised points x, as FP32."""
+        with torch.autocast("cuda", dtype=torch.float16, enabled=self.sdf_fp16 and x.is_cuda):
+            sdf, feat = self.net(x)
+            grad, = torch.autograd.grad(sdf.sum(), x, create_graph=create_graph)
+        return sdf.float(), feat.float(), grad.float()
+
     def _fill_bank(self) -> None:
         """Renders every chunk once with the current network (rf_rendering.py:558-604)."""
         x = ((self.points - self.center) / self.scale).requires_grad_(True)
-        sdf, feat = self.net(x)
-        grad, = torch.autograd.grad(sdf.sum(), x)
+        sdf, feat, grad = self._sdf(x, create_graph=False)
         with torch.no_grad():
             normals, sig = self._render_inputs(sdf.detach(), feat.detach(), grad)
             P = self.R * self.T
@@ -237,8 +247,7 @@ class Stage1RFStep(_Graphable):
         self.opt.zero_grad(set_to_none=False)
         A, S = self.tx.shape[0], self.chirp.num_samples
         x = ((self.points - self.center) / self.scale).requires_grad_(True)
-        sdf, feat = self.net(x)
-        grad, = torch.autograd.grad(sdf.sum(), x, create_graph=True)
+        sdf, feat, grad = self._sdf(x, create_graph=True)
         normals, sig = self._render_inputs(sdf, feat, grad)
         P = self.R * self.T
         N = self.voxels.shape[0]
