@@ -172,6 +172,29 @@ def fp32_peak_tflops(dev) -> float:
     return best
 
 
+def horner_ceiling_tflops(dev) -> float:
+    """Measured rate of the MIXED forward's Horner loop alone (geraf_rf_horner_probe:
+    no per-(voxel, antenna) set-up), the ceiling of that loop's instruction form."""
+    import torch
+
+    from geraf_b200 import _lib
+
+    lib = _lib.load()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    blocks, threads, rows = sms * 3, 128, 256
+    sink = torch.empty(blocks * threads, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    best = 0.0
+    for _ in range(4):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        _lib.check(lib.geraf_rf_horner_probe(blocks, threads, rows, sink.data_ptr(), stream), "horner probe")
+        e.record()
+        e.synchronize()
+        best = max(best, blocks * threads * rows * 16384 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    return best
+
+
 def make_mf_workload(name, rank, world, dev, seed):
     import numpy as np
     import torch
@@ -201,23 +224,25 @@ def mf_call(wl, out_r, out_i, precision, voxel=None, N=None, tuning=None):
                              wl["S"], ch.adc_sample_rate, ch.As_sci, n, precision=precision, tuning=tuning)
 
 
-def autotune_mf_forward(wl, precision, dev, subset=131072):
-    """Runs the autotuner for the headline call (untimed): launch shapes are timed
-    on a voxel subset; the winner is recorded under the full problem's key."""
+def autotune_mf_forward(wl, precision, dev, antenna_fraction=8):
+    """Runs the autotuner for the headline call (untimed).  Launch shapes are timed
+    on every voxel and a leading 1/8 of the antennas, so the grid, the waves per
+    SM and the antenna split match the full call while each candidate takes an
+    eighth of its time; the winner is recorded under the full problem's key."""
     import torch
 
     from geraf_b200 import _lib, autotune
 
     mode = _lib.MODE_MIXED if precision == "mixed" else _lib.MODE_PLAIN
-    n = min(subset, wl["N"])
-    vsub = wl["voxel"][:, :n].contiguous()
-    yr = torch.empty(n, device=dev)
-    yi = torch.empty(n, device=dev)
+    a_sub = max(1, wl["A"] // antenna_fraction)
+    sub = dict(wl, A=a_sub, real=wl["real"][:a_sub], imag=wl["imag"][:a_sub], tx=wl["tx"][:a_sub],
+               rx=wl["rx"][:a_sub])
+    yr = torch.empty(wl["N"], device=dev)
+    yi = torch.empty(wl["N"], device=dev)
     cands = [c for c in autotune.mf_forward_candidates(mode)
-             if c["stage_rows"] in ((4, 8) if precision == "mixed" else (8, 16))]
+             if c["threads"] >= 128 and c["stage_rows"] in ((4, 8) if precision == "mixed" else (8, 16))]
     best, results = autotune.tune("mf_forward", (wl["A"], wl["S"], wl["N"]), mode,
-                                  lambda t: mf_call(wl, yr, yi, precision, voxel=vsub, N=n, tuning=t),
-                                  cands, iters=1)
+                                  lambda t: mf_call(sub, yr, yi, precision, tuning=t), cands, iters=1)
     return best, len(results)
 
 
@@ -331,6 +356,7 @@ def run_ours(args):
     e2e_value = world * triples / (e2e_ms * 1e-3) / 1e9
 
     peak = fp32_peak_tflops(dev)
+    ceiling = horner_ceiling_tflops(dev) if args.precision == "mixed" else None
     achieved = FLOPS_PER_TRIPLE * triples / (kms * 1e-3) / 1e12
     traffic = read_profile_traffic(args.workload)
     launches = launches_per_mf_call(wl, args.precision) * args.steps
@@ -360,6 +386,13 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clock_info,
     }
+    if ceiling is not None:
+        # The Horner loop alone, without the per-(voxel, antenna) set-up: the ceiling of
+        # the kernel's instruction form, below the FMA-rate peak (operand fetch).
+        line["roofline"]["loop_ceiling"] = {
+            "value": round(ceiling, 3), "unit": "TFLOP/s", "frac_of_peak": round(ceiling / peak, 4),
+            "kernel_frac_of_ceiling": round(achieved / ceiling, 4),
+            "source": "geraf_rf_horner_probe (the forward's packed Horner loop alone) in this process"}
 
     wanted = set() if args.no_extras else {x.strip() for x in args.extras.split(",") if x.strip()}
     if rank == 0 and wanted:

@@ -867,6 +867,28 @@ cudaError_t launch_finalize_partials(int dtype, const float2* partial, int split
   return cudaGetLastError();
 }
 
+// Resident blocks per SM of the forward kernel at this shape, from the
+// occupancy calculator (registers and dynamic shared memory both count); the
+// thread-count bound when no device answers (workspace queries on a host
+// without a GPU never launch).
+int fwd_blocks_per_sm(const MfArgs& a, const Tuning& t) {
+  Tuning one = t;
+  one.splits = 1;
+  const FwdShape s = fwd_shape(a, one);
+  const void* fn = a.dtype == kF64   ? fwd_kernel_ptr<double>(a.mode, s.vpt)
+                   : a.dtype == kF16 ? fwd_kernel_ptr<__half>(a.mode, s.vpt)
+                                     : fwd_kernel_ptr<float>(a.mode, s.vpt);
+  int n = 0;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(s.smem)) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, s.threads, s.smem) != cudaSuccess ||
+      n <= 0) {
+    cudaGetLastError();
+    return std::max(1, 1024 / t.threads);
+  }
+  return n;
+}
+
 Tuning mf_forward_resolve(const MfArgs& a, const Tuning& req) {
   if (a.mode == kNufft) return mf_nufft_forward_resolve(a, req);
   Tuning t = req;
@@ -888,8 +910,9 @@ Tuning mf_forward_resolve(const MfArgs& a, const Tuning& req) {
     const int64_t vtiles = (a.N + static_cast<int64_t>(t.threads) * t.items - 1) /
                            (static_cast<int64_t>(t.threads) * t.items);
     const DeviceInfo dev = current_device_info();
-    const int per_sm = std::max(1, 1024 / t.threads);
-    t.splits = a.mode == kPlain ? 1 : pick_splits(vtiles, per_sm, dev.sm_count, rows_total);
+    t.splits = a.mode == kPlain
+                   ? 1
+                   : pick_splits(vtiles, fwd_blocks_per_sm(a, t), dev.sm_count, rows_total);
   }
   t.splits = static_cast<int>(std::min<int64_t>(std::max(t.splits, 1), rows_total));
   if (t.chunk <= 0) t.chunk = 16;

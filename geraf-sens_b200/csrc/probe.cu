@@ -33,6 +33,69 @@ __global__ void __launch_bounds__(256) fma_probe_kernel(float* sink, int iters, 
   if (s == 1234.5f) sink[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the chains live
 }
 
+// The MIXED matched-filter forward's inner loop on its own: 4 packed voxel
+// pairs per thread run the Horner recurrence P <- P z + s over `rows` rows of
+// 256 samples, broadcast from shared memory in the duplicated (s, s) layout,
+// with the per-(voxel, antenna) phase set-up left out (the phasors are fixed
+// per thread).  Its rate is the ceiling of that loop's instruction form: every
+// packed FMA of the complex step reads two or three register operands that
+// the instruction before it did not, while the FMA-rate probe above reuses two
+// of its three, so this loop stays below the FMA peak however it is scheduled.
+__global__ void __launch_bounds__(128) horner_probe_kernel(float* sink, int rows, float seed) {
+  constexpr int kLen = 256;
+  constexpr int kPairs = 4;
+  __shared__ __align__(16) float2 dup[2][kLen];
+  for (int i = threadIdx.x; i < kLen; i += blockDim.x) {
+    const float v = 1.0e-3f * static_cast<float>(i % 17) - 8.0e-3f;
+    dup[0][i] = make_float2(v, v);
+    dup[1][i] = make_float2(-v, -v);
+  }
+  __syncthreads();
+  float2 zr[kPairs], zi[kPairs], nzi[kPairs], acc[kPairs];
+#pragma unroll
+  for (int q = 0; q < kPairs; ++q) {
+    float s0, c0, s1, c1;
+    sincospif(seed * static_cast<float>(threadIdx.x + 1) * 1.0e-3f + 0.1f * q, &s0, &c0);
+    sincospif(seed * static_cast<float>(threadIdx.x + 2) * 1.0e-3f + 0.13f * q, &s1, &c1);
+    zr[q] = make_float2(c0, c1);
+    zi[q] = make_float2(-s0, -s1);
+    nzi[q] = make_float2(s0, s1);
+    acc[q] = make_float2(0.0f, 0.0f);
+  }
+  for (int r = 0; r < rows; ++r) {
+    float2 pr[kPairs], pi[kPairs];
+#pragma unroll
+    for (int q = 0; q < kPairs; ++q) pr[q] = pi[q] = make_float2(0.0f, 0.0f);
+#pragma unroll 2
+    for (int n = kLen - 2; n >= 0; n -= 2) {
+      const float4 a = *reinterpret_cast<const float4*>(&dup[0][n]);
+      const float4 b = *reinterpret_cast<const float4*>(&dup[1][n]);
+      const float2 sr[2] = {make_float2(a.z, a.w), make_float2(a.x, a.y)};
+      const float2 si[2] = {make_float2(b.z, b.w), make_float2(b.x, b.y)};
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+#pragma unroll
+        for (int q = 0; q < kPairs; ++q) {
+          const float2 t1 = geraf::ffma2(pi[q], nzi[q], sr[h]);
+          const float2 t2 = geraf::ffma2(pi[q], zr[q], si[h]);
+          const float2 npr = geraf::ffma2(pr[q], zr[q], t1);
+          pi[q] = geraf::ffma2(pr[q], zi[q], t2);
+          pr[q] = npr;
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kPairs; ++q) {
+      acc[q].x += pr[q].x + pi[q].y;
+      acc[q].y += pi[q].x + pr[q].y;
+    }
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int q = 0; q < kPairs; ++q) s += acc[q].x + acc[q].y;
+  if (s == 1234.5f) sink[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the loop live
+}
+
 }  // namespace
 
 // Enqueues blocks x threads threads of `iters` iterations x 16 FMAs each
@@ -43,5 +106,17 @@ GERAF_EXPORT int32_t geraf_rf_fma_probe(int32_t blocks, int32_t threads, int32_t
     return GERAF_ERR_INVALID_ARGUMENT;
   }
   fma_probe_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(sink, iters, 0.5f);
+  return cudaGetLastError() == cudaSuccess ? GERAF_OK : GERAF_ERR_CUDA;
+}
+
+// Enqueues blocks x threads (threads <= 128) threads of the Horner loop over
+// `rows` rows of 256 samples x 8 voxels (flops = blocks * threads * rows * 16384).
+// `sink` needs blocks*threads floats.
+GERAF_EXPORT int32_t geraf_rf_horner_probe(int32_t blocks, int32_t threads, int32_t rows,
+                                           float* sink, void* stream) {
+  if (blocks <= 0 || threads <= 0 || threads > 128 || rows <= 0 || sink == nullptr) {
+    return GERAF_ERR_INVALID_ARGUMENT;
+  }
+  horner_probe_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(sink, rows, 0.5f);
   return cudaGetLastError() == cudaSuccess ? GERAF_OK : GERAF_ERR_CUDA;
 }

@@ -95,6 +95,14 @@ const char* geraf_rf_build_info(void);
  * the RF kernels; no counterpart in the reference. */
 int32_t geraf_rf_fma_probe(int32_t blocks, int32_t threads, int32_t iters, float* sink,
                            void* stream);
+/* Enqueues blocks x threads threads (threads <= 128) of the MIXED matched
+ * filter forward's Horner loop alone -- 8 voxels per thread in packed pairs,
+ * `rows` rows of 256 shared-memory samples, no per-(voxel, antenna) phase
+ * set-up -- i.e. blocks*threads*rows*16384 flops, for timing by the caller.
+ * The ceiling of that loop's instruction form, reported beside the FMA-rate
+ * roofline; `sink` as above.  No counterpart in the reference. */
+int32_t geraf_rf_horner_probe(int32_t blocks, int32_t threads, int32_t rows, float* sink,
+                              void* stream);
 /* Reads, and with reset != 0 clears, the device status word of the current
  * device: GERAF_OK, or the code a kernel raised -- GERAF_ERR_DEVICE_TIMEOUT
  * (a bounded wait gave up), GERAF_ERR_INVALID_ARGUMENT (malformed ragged
