@@ -234,9 +234,7 @@ def autotune_mf_forward(wl, precision, dev, antenna_fraction=8):
     from geraf_b200 import _lib, autotune
 
     mode = _lib.MODE_MIXED if precision == "mixed" else _lib.MODE_PLAIN
-    a_sub = max(1, wl["A"] // antenna_fraction)
-    sub = dict(wl, A=a_sub, real=wl["real"][:a_sub], imag=wl["imag"][:a_sub], tx=wl["tx"][:a_sub],
-               rx=wl["rx"][:a_sub])
+    sub = antenna_subset(wl, max(1, wl["A"] // antenna_fraction))
     yr = torch.empty(wl["N"], device=dev)
     yi = torch.empty(wl["N"], device=dev)
     cands = [c for c in autotune.mf_forward_candidates(mode)
@@ -508,22 +506,52 @@ def _stage1_extra(args, dev) -> dict:
                             **res}}
 
 
+def antenna_subset(wl, a_sub):
+    """The workload restricted to its leading ``a_sub`` antennas (all voxels)."""
+    return dict(wl, A=a_sub, real=wl["real"][:a_sub], imag=wl["imag"][:a_sub], tx=wl["tx"][:a_sub],
+                rx=wl["rx"][:a_sub])
+
+
 def _plain_extra(wl, dev) -> dict:
+    """PLAIN form (the reference's FP32 expressions, one sincos per triple) on every
+    voxel and a leading antenna subset sized to about 1.5 s, so the grid is the
+    full call's; forward and adjoint (the adjoint on every antenna and sample and
+    a voxel subset: its threads are the (antenna, sample) pairs)."""
     import torch
 
     from geraf_b200 import autotune
+    from geraf_b200.ops.RFMatchedFilter import _C as mfc
 
     res = {}
     A, S, N = wl["A"], wl["S"], wl["N"]
-    # PLAIN form on a voxel subset (it evaluates sinf/cosf per triple)
-    n_sub = min(N, 16384)
-    vsub = wl["voxel"][:, :n_sub].contiguous()
-    pr = torch.empty(n_sub, device=dev)
-    pi = torch.empty(n_sub, device=dev)
-    mf_call(wl, pr, pi, "plain", voxel=vsub, N=n_sub)
-    ms = autotune.time_call(lambda: mf_call(wl, pr, pi, "plain", voxel=vsub, N=n_sub), iters=1, warmup=0)
-    res["plain_form"] = {"value": round(float(A) * S * n_sub / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
-                         "voxels": n_sub, "ms": round(ms, 2)}
+    ch = wl["chirp"]
+    pr = torch.empty(N, device=dev)
+    pi = torch.empty(N, device=dev)
+    a_cal = min(A, 16)
+    ms = autotune.time_call(lambda: mf_call(antenna_subset(wl, a_cal), pr, pi, "plain"), iters=1, warmup=1)
+    a_sub = int(min(A, max(a_cal, a_cal * 1500.0 / max(ms, 1e-3))))
+    sub = antenna_subset(wl, a_sub)
+    ms = autotune.time_call(lambda: mf_call(sub, pr, pi, "plain"), iters=1, warmup=0)
+    res["plain_form"] = {"value": round(float(a_sub) * S * N / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                         "sample": f"{N} voxels x {a_sub} antennas x {S} samples", "ms": round(ms, 2)}
+    g_r = torch.randn(N, device=dev)
+    g_i = torch.randn(N, device=dev)
+    h_r = torch.empty((A, S), device=dev)
+    h_i = torch.empty((A, S), device=dev)
+
+    def adj(n_sub):
+        v = wl["voxel"][:, :n_sub].contiguous()
+        return lambda: mfc.MatchedFilter_backward_realimag(g_r[:n_sub], g_i[:n_sub], wl["real"], wl["imag"],
+                                                           wl["tx"], wl["rx"], h_r, h_i, v, A, S,
+                                                           ch.adc_sample_rate, ch.As_sci, n_sub,
+                                                           precision="plain")
+
+    n_cal = min(N, 64)
+    ms = autotune.time_call(adj(n_cal), iters=1, warmup=1)
+    n_sub = int(min(N, max(n_cal, n_cal * 1500.0 / max(ms, 1e-3))))
+    ms = autotune.time_call(adj(n_sub), iters=1, warmup=0)
+    res["plain_adjoint"] = {"value": round(float(A) * S * n_sub / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                            "sample": f"{A} antennas x {S} samples x {n_sub} voxels", "ms": round(ms, 2)}
     return res
 
 
@@ -697,6 +725,113 @@ def cpu_leg(wl, out_r, out_i, dev):
 
 
 # ---------------------------------------------------------------------------
+def reference_cuda_leg(args, w) -> dict:
+    """The reference's own CUDA kernels -- the unmodified extensions, built for
+    sm_100a into oracle/_ref by oracle/build_ref.py -- timed with CUDA events on
+    this GPU, through their own ``_C`` entry points:
+
+    - MF forward (one thread per voxel looping over antennas x samples,
+      MatchedFilter_cuda_kernel.cu:65-115): every voxel of the workload and a
+      leading subset of its antennas, so the grid is the full call's and the cost
+      per voxel-antenna-sample is unchanged;
+    - MF adjoint (one thread per antenna x sample looping over voxels, :171-220):
+      every antenna and sample and a voxel subset, for the same reason;
+    - tracer forward + adjoint onto normals and sigmas (SignalTracer_cuda_kernel.cu:
+      351-587) on the 64-antenna x 4096-ray x 128-sample tracer workload, as is.
+
+    Inputs are seeded Gaussian IF and gradients (the cost does not depend on the
+    values) and the random-init SDF tracer scene."""
+    import torch
+
+    from geraf_b200.sdf import tracer_workload
+    from oracle import build_ref
+
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    try:
+        mf = build_ref.load("RFMatchedFilter")
+        st = build_ref.load("RFSignalTracer")
+    except Exception as exc:  # noqa: BLE001 - reported, not fatal to the CPU arm
+        return {"unavailable": f"reference extensions not loadable: {exc}"}
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ch = w["chirp"]
+    A, S, N = w["tx"].shape[0], ch.num_samples, w["voxel"].shape[1]
+    gen = torch.Generator(device=dev).manual_seed(args.seed)
+    re = torch.randn((A, S), device=dev, generator=gen)
+    im = torch.randn((A, S), device=dev, generator=gen)
+    tx = torch.tensor(w["tx"], device=dev, dtype=torch.float32)
+    rx = torch.tensor(w["rx"], device=dev, dtype=torch.float32)
+    vox = torch.tensor(w["voxel"], device=dev, dtype=torch.float32).contiguous()
+
+    def timed(fn, iters=1):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(iters):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / iters
+
+    out = {"build": "oracle/build_ref.py: the reference's _C sources, unmodified, -gencode sm_100a",
+           "unit": UNIT}
+    # MF forward: all N voxels, a_sub antennas (sized from a short calibration to ~2 s)
+    yr = torch.empty(N, device=dev)
+    yi = torch.empty(N, device=dev)
+
+    def fwd(a_sub):
+        return lambda: mf.MatchedFilter_forward(re[:a_sub], im[:a_sub], tx[:a_sub], rx[:a_sub], yr, yi, vox,
+                                                a_sub, S, ch.adc_sample_rate, ch.As_sci, N)
+
+    a_cal = min(A, 8)
+    ms = timed(fwd(a_cal))
+    a_sub = int(min(A, max(a_cal, a_cal * 2000.0 / max(ms, 1e-3))))
+    ms = timed(fwd(a_sub))
+    out["mf_forward"] = {"value": round(float(a_sub) * S * N / (ms * 1e-3) / 1e9, 3), "ms": round(ms, 2),
+                         "sample": f"{N} voxels x {a_sub} antennas x {S} samples"}
+    # MF adjoint: all A x S threads, n_sub voxels
+    gr = torch.randn(N, device=dev, generator=gen)
+    gi = torch.randn(N, device=dev, generator=gen)
+    hr = torch.empty((A, S), device=dev)
+    hi = torch.empty((A, S), device=dev)
+
+    def adj(n_sub):
+        v = vox[:, :n_sub].contiguous()
+        return lambda: mf.MatchedFilter_backward_realimag(gr[:n_sub], gi[:n_sub], re, im, tx, rx, hr, hi, v,
+                                                          A, S, ch.adc_sample_rate, ch.As_sci, n_sub)
+
+    n_cal = min(N, 64)
+    ms = timed(adj(n_cal))
+    n_sub = int(min(N, max(n_cal, n_cal * 2000.0 / max(ms, 1e-3))))
+    ms = timed(adj(n_sub))
+    out["mf_adjoint"] = {"value": round(float(A) * S * n_sub / (ms * 1e-3) / 1e9, 3), "ms": round(ms, 2),
+                         "sample": f"{A} antennas x {S} samples x {n_sub} voxels"}
+    # tracer forward + adjoint (normals, sigmas) on the tracer workload
+    tw = tracer_workload(device=dev, seed=args.seed)
+    At, P, St = tw["A"], tw["P"], tw["chirp"].num_samples
+    cfg = tw["radar_cfg"]
+    xr = torch.empty((At, St), device=dev)
+    xi = torch.empty((At, St), device=dev)
+    gxr = torch.randn((At, St), device=dev, generator=gen)
+    gxi = torch.randn((At, St), device=dev, generator=gen)
+    gn = torch.empty((P, 3), device=dev)
+    gs = torch.empty((At, P), device=dev)
+
+    def tr_step():
+        st.SignalTracer_forward(tw["normals"], tw["sigmas"], tw["points"], tw["tx"], tw["rx"], tw["inbounds"],
+                                xr, xi, St, cfg["adcSampleRate"], cfg["fc_start"], cfg["As_sci"], At, P)
+        st.SignalTracer_backward_normal_sigma(gxr, gxi, tw["normals"], tw["sigmas"], tw["points"], tw["tx"],
+                                              tw["rx"], tw["inbounds"], gn, gs, St, cfg["adcSampleRate"],
+                                              cfg["fc_start"], cfg["As_sci"], At, P)
+
+    ms = timed(tr_step)
+    out["tracer"] = {"workload": f"{At} antennas x {tw['rays']} rays x {P // tw['rays']} samples, S={St}",
+                     "rays_per_s": round(At * tw["rays"] / (ms * 1e-3), 1), "ms": round(ms, 3),
+                     "unit": "rays/s (ray = ray x antenna pair), forward + adjoint onto normals and sigmas"}
+    return out
+
+
 def run_reference(args):
     """Times the reference's arithmetic on the host cores (the FP32
     reference-order oracle port; the reference ships no CPU implementation)."""
@@ -746,6 +881,8 @@ def run_reference(args):
                          "sample": sample},
         "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if not args.no_extras:
+        line["reference_cuda"] = reference_cuda_leg(args, w)
     print(json.dumps(line), flush=True)
 
 

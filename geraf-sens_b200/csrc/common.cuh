@@ -233,6 +233,12 @@ __device__ __forceinline__ float2 cis_cycles(float x) {
   return make_float2(c, s);
 }
 
+// cosf(x) and sinf(x) from one sincosf call.  sincosf returns the same bits as
+// the two separate calls for every FP32 input -- geraf_rf_sincos_identity_check
+// compares all 2^32 inputs on the device -- so the PLAIN kernels keep the
+// reference's results while the argument reduction is done once.
+__device__ __forceinline__ void cos_sin(float x, float* c, float* s) { sincosf(x, s, c); }
+
 // Packed FP32 fused multiply-add on two lanes (fma.rn.f32x2, sm_100+): one
 // instruction for two independent FMAs, halving the issue slots of FMA-bound
 // loops.  Results are those of two fmaf calls.

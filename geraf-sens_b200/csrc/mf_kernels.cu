@@ -309,8 +309,9 @@ __global__ void __launch_bounds__(256) mf_fwd_plain_kernel(const MfFwdP<T> p) {
         float acc_r = ar[j], acc_i = ai[j];
         for (int n = 0; n < S; ++n) {
           const float phase = base_phase + kn[n] * tau;
-          const float cos_phase = cosf(phase);
-          const float neg_sin_phase = -sinf(phase);
+          float cos_phase, sin_phase;
+          cos_sin(phase, &cos_phase, &sin_phase);
+          const float neg_sin_phase = -sin_phase;
           const float sample_real = static_cast<float>(rowr[n]);
           const float sample_imag = static_cast<float>(rowi[n]);
           acc_r += cos_phase * sample_real - neg_sin_phase * sample_imag;
@@ -508,12 +509,15 @@ __global__ void __launch_bounds__(128) mf_bwd_plain_kernel(const MfBwdP<T> p) {
       for (int i = 0; i < count; ++i) {
         const float tau = s_tau[i];
         const float phase = 2.0f * kPiF * kMfStartFrequency * tau + kn * tau;
-        const float cos_phase = cosf(phase);
-        const float neg_sin_phase = -sinf(phase);
+        float cos_phase, sin_phase;
+        cos_sin(phase, &cos_phase, &sin_phase);
+        const float neg_sin_phase = -sin_phase;
         const float grad_real_out = s_gr[i];
         const float grad_imag_out = s_gi[i];
-        acc_r += cos_phase * grad_real_out + neg_sin_phase * grad_imag_out;
-        acc_i += (-neg_sin_phase) * grad_real_out + cos_phase * grad_imag_out;
+        // The reference's expressions with the FMA contraction its build makes
+        // (identified against its outputs): the cos product is fused in both.
+        acc_r = __fadd_rn(acc_r, __fmaf_rn(cos_phase, grad_real_out, __fmul_rn(neg_sin_phase, grad_imag_out)));
+        acc_i = __fadd_rn(acc_i, __fmaf_rn(cos_phase, grad_imag_out, __fmul_rn(sin_phase, grad_real_out)));
       }
     }
     __syncthreads();
@@ -560,8 +564,9 @@ __global__ void __launch_bounds__(256) mf_fft_fwd_kernel(const MfFftP<T> p) {
     if (range_bin < 0 || range_bin >= num_range_bins) continue;
     const float tau = distance / kSpeedOfLight;
     const float phase = 2.0f * kPiF * kMfStartFrequency * tau;
-    const float cos_phase = cosf(phase);
-    const float neg_sin_phase = -sinf(phase);
+    float cos_phase, sin_phase;
+    cos_sin(phase, &cos_phase, &sin_phase);
+    const float neg_sin_phase = -sin_phase;
     const float sample_real = ld_f(p.real, a * p.bins + range_bin);
     const float sample_imag = ld_f(p.imag, a * p.bins + range_bin);
     acc_r += cos_phase * sample_real - neg_sin_phase * sample_imag;
@@ -609,12 +614,15 @@ __global__ void __launch_bounds__(128) mf_fft_bwd_kernel(const MfFftP<T> p) {
         if (s_bin[i] != b) continue;
         const float tau = s_tau[i];
         const float phase = 2.0f * kPiF * kMfStartFrequency * tau;
-        const float cos_phase = cosf(phase);
-        const float neg_sin_phase = -sinf(phase);
+        float cos_phase, sin_phase;
+        cos_sin(phase, &cos_phase, &sin_phase);
+        const float neg_sin_phase = -sin_phase;
         const float grad_real_out = s_gr[i];
         const float grad_imag_out = s_gi[i];
-        acc_r += cos_phase * grad_real_out + neg_sin_phase * grad_imag_out;
-        acc_i += (-neg_sin_phase) * grad_real_out + cos_phase * grad_imag_out;
+        // The reference's expressions with the FMA contraction its build makes
+        // (identified against its outputs): the cos product is fused in both.
+        acc_r = __fadd_rn(acc_r, __fmaf_rn(cos_phase, grad_real_out, __fmul_rn(neg_sin_phase, grad_imag_out)));
+        acc_i = __fadd_rn(acc_i, __fmaf_rn(cos_phase, grad_imag_out, __fmul_rn(sin_phase, grad_real_out)));
       }
     }
     __syncthreads();

@@ -96,6 +96,24 @@ __global__ void __launch_bounds__(128) horner_probe_kernel(float* sink, int rows
   if (s == 1234.5f) sink[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the loop live
 }
 
+// Counts the FP32 inputs, over all 2^32 bit patterns, for which sincosf differs
+// in any bit from separate sinf and cosf calls: the PLAIN kernels rely on there
+// being none.
+__global__ void sincos_identity_kernel(unsigned long long* mismatches) {
+  unsigned long long local = 0;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < (1ull << 32);
+       i += stride) {
+    const float x = __uint_as_float(static_cast<unsigned int>(i));
+    float s1, c1;
+    sincosf(x, &s1, &c1);
+    const float s0 = sinf(x);
+    const float c0 = cosf(x);
+    if (__float_as_uint(s0) != __float_as_uint(s1) || __float_as_uint(c0) != __float_as_uint(c1)) ++local;
+  }
+  if (local != 0) atomicAdd(mismatches, local);
+}
+
 }  // namespace
 
 // Enqueues blocks x threads threads of `iters` iterations x 16 FMAs each
@@ -118,5 +136,13 @@ GERAF_EXPORT int32_t geraf_rf_horner_probe(int32_t blocks, int32_t threads, int3
     return GERAF_ERR_INVALID_ARGUMENT;
   }
   horner_probe_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(sink, rows, 0.5f);
+  return cudaGetLastError() == cudaSuccess ? GERAF_OK : GERAF_ERR_CUDA;
+}
+
+// Adds to *mismatches (device memory, zeroed by the caller) the number of FP32
+// inputs for which sincosf and separate sinf / cosf calls differ in any bit.
+GERAF_EXPORT int32_t geraf_rf_sincos_identity_check(unsigned long long* mismatches, void* stream) {
+  if (mismatches == nullptr) return GERAF_ERR_INVALID_ARGUMENT;
+  sincos_identity_kernel<<<148 * 16, 256, 0, static_cast<cudaStream_t>(stream)>>>(mismatches);
   return cudaGetLastError() == cudaSuccess ? GERAF_OK : GERAF_ERR_CUDA;
 }

@@ -112,8 +112,10 @@ __global__ void __launch_bounds__(128) tracer_fwd_plain_kernel(const TrP<T> p) {
       for (int i = 0; i < count; ++i) {
         if (!s_valid[i]) continue;
         const float phase = __fmul_rn(w, s_tau[i]);
-        acc_r += s_amp[i] * cosf(phase);
-        acc_i += s_amp[i] * sinf(phase);
+        float c, sn;
+        cos_sin(phase, &c, &sn);
+        acc_r += s_amp[i] * c;
+        acc_i += s_amp[i] * sn;
       }
     }
     __syncthreads();
@@ -440,8 +442,8 @@ __global__ void __launch_bounds__(128) tracer_bwd_plain_kernel(const TrP<T> p) {
         const float sample_time = static_cast<float>(n) / p.fs;
         const float omega = adjoint_phase_rate<T>(p.f0, p.As, sample_time);
         const float phase = __fmul_rn(omega, tau);
-        const float phase_real = cosf(phase);
-        const float phase_imag = sinf(phase);
+        float phase_real, phase_imag;
+        cos_sin(phase, &phase_real, &phase_imag);
         const float gro = static_cast<float>(rowr[n]);
         const float gio = static_cast<float>(rowi[n]);
         const float grad_real = gro * phase_real;

@@ -69,6 +69,7 @@ SIGNATURES = {
     "geraf_rf_device_status": (_i32, [_vp, _i32, ctypes.POINTER(_i32)]),
     "geraf_rf_fma_probe": (_i32, [_i32, _i32, _i32, _vp, _vp]),
     "geraf_rf_horner_probe": (_i32, [_i32, _i32, _i32, _vp, _vp]),
+    "geraf_rf_sincos_identity_check": (_i32, [_vp, _vp]),
     "geraf_mf_forward_workspace_bytes": (_i32, [_i64, _i64, _i64, _i32, _i32, _tp, _szp]),
     "geraf_mf_forward": (
         _i32,

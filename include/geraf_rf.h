@@ -103,6 +103,14 @@ int32_t geraf_rf_fma_probe(int32_t blocks, int32_t threads, int32_t iters, float
  * roofline; `sink` as above.  No counterpart in the reference. */
 int32_t geraf_rf_horner_probe(int32_t blocks, int32_t threads, int32_t rows, float* sink,
                               void* stream);
+/* Enqueues a check of every FP32 input (all 2^32 bit patterns): adds to
+ * *mismatches (device memory, zeroed by the caller) the number of inputs for
+ * which sincosf differs in any bit from separate sinf and cosf calls.  The
+ * PLAIN kernels take cos and sin of each phase from one sincosf call where the
+ * reference calls cosf and sinf (MatchedFilter_cuda_kernel.cu:60-63,
+ * SignalTracer_cuda_kernel.cu:442-443, 555-556); their bit-exactness rests on
+ * this count being zero.  No counterpart in the reference. */
+int32_t geraf_rf_sincos_identity_check(unsigned long long* mismatches, void* stream);
 /* Reads, and with reset != 0 clears, the device status word of the current
  * device: GERAF_OK, or the code a kernel raised -- GERAF_ERR_DEVICE_TIMEOUT
  * (a bounded wait gave up), GERAF_ERR_INVALID_ARGUMENT (malformed ragged

@@ -24,7 +24,7 @@ def header_functions():
 def test_header_parses():
     fns = header_functions()
     assert "geraf_mf_forward" in fns and "geraf_tracer_backward" in fns
-    assert len(fns) == 22
+    assert len(fns) == 23
 
 
 def test_library_exports_every_declared_symbol():

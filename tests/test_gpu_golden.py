@@ -42,12 +42,14 @@ def test_mf_plain_matches_reference(cuda, name, parity_log):
                          A, S, g["fs"], g["As"], "plain", dt)
     e_f = rel_l2(yr + 1j * yi, ref)
     e_b = rel_l2(hr + 1j * hi, g["grad_real"] + 1j * g["grad_imag"])
+    bx_f = bitexact(np.r_[yr, yi], np.r_[g["out_real"], g["out_imag"]])
+    bx_b = bitexact(np.r_[hr.ravel(), hi.ravel()], np.r_[g["grad_real"].ravel(), g["grad_imag"].ravel()])
     parity_log(f"mf_plain_vs_reference[{name}]", forward_rel_l2=e_f, adjoint_rel_l2=e_b,
-               forward_bitexact=bitexact(np.r_[yr, yi], np.r_[g["out_real"], g["out_imag"]]),
-               adjoint_bitexact=bitexact(np.r_[hr.ravel(), hi.ravel()],
-                                         np.r_[g["grad_real"].ravel(), g["grad_imag"].ravel()]))
+               forward_bitexact=bx_f, adjoint_bitexact=bx_b)
     assert e_f < tol
     assert e_b < tol
+    # same FP32 expressions, same per-output order: every output bit equals the reference's
+    assert bx_f == 1.0 and bx_b == 1.0
 
 
 @pytest.mark.parametrize("name", [c for c in golden_cases("mf_") if "fft" not in c])
@@ -101,6 +103,11 @@ def test_tracer_plain_matches_reference(cuda, name, parity_log):
                grad_bitexact=bitexact(np.r_[gn[inb].ravel(), gs[:, inb].ravel()],
                                       np.r_[g["grad_normals"][inb].ravel(), g["grad_sigmas"][:, inb].ravel()]))
     assert rel_l2(xr + 1j * xi, g["out_real"] + 1j * g["out_imag"]) < PLAIN_TOL
+    if dt == torch.float32:
+        # FP32 inputs: every output bit equals the reference's
+        assert bitexact(np.r_[xr.ravel(), xi.ravel()], np.r_[g["out_real"].ravel(), g["out_imag"].ravel()]) == 1.0
+        assert bitexact(np.r_[gn[inb].ravel(), gs[:, inb].ravel()],
+                        np.r_[g["grad_normals"][inb].ravel(), g["grad_sigmas"][:, inb].ravel()]) == 1.0
     # the reference leaves out-of-bounds entries unwritten (NaN-prefilled); this library writes 0
     assert np.all(np.isnan(g["grad_normals"][~inb])) and np.all(gn[~inb] == 0)
     assert np.all(gs[:, ~inb] == 0)
