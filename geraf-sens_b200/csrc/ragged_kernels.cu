@@ -14,8 +14,9 @@
 // blocks then take items from an atomic counter until none are left, so
 // antennas with 512 rays and antennas with 8192 rays load-balance; a finish
 // pass sums each antenna's item partials in item order (deterministic).
-// Adjoint: one thread per point; a point belongs to one antenna, so the
-// gradients need no reduction across antennas.
+// Adjoint: a point belongs to one antenna, so its gradients need no reduction
+// across antennas; blocks screen tiles of points and deal the live ones out
+// over their threads.
 #include <algorithm>
 
 #include "common.cuh"
@@ -277,40 +278,165 @@ __global__ void ragged_finish_kernel(const RgP<T> p) {
   }
 }
 
-// Adjoint: thread = point.  Residual rows of the antennas a block touches are
-// staged in shared memory when there are few of them (points are grouped by
-// antenna, so a block of points usually belongs to one antenna).
-template <typename T, bool WITH_POINTS>
-__global__ void __launch_bounds__(128) ragged_bwd_kernel(const RgP<T> p, int ld, int max_rows) {
-  extern __shared__ __align__(16) float srow[];  // [max_rows][2][ld]
-  __shared__ long long s_a0, s_a1;
-  const int64_t pi = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-  const bool inside = pi < p.P;
-
-  int64_t a = 0;
-  bool owned = false;
-  if (inside) {
-    int64_t lo = 0, hi = p.A;  // last a with offsets[a] <= pi
-    while (hi - lo > 1) {
-      const int64_t mid = (lo + hi) >> 1;
-      if (p.offsets[mid] <= pi) lo = mid;
-      else hi = mid;
-    }
-    a = lo;
-    owned = p.A > 0 && p.offsets[a] <= pi && pi < p.offsets[a + 1];
-    if (!owned && p.status != nullptr) atomicExch(p.status, kStatusBadOffsets);
+// Antenna owning point pi: the last a with offsets[a] <= pi.  *owned is false
+// when the offsets do not cover pi (malformed input).
+__device__ __forceinline__ int64_t point_antenna(const int64_t* offsets, int64_t A, int64_t pi,
+                                                 bool* owned) {
+  int64_t lo = 0, hi = A;
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (offsets[mid] <= pi) lo = mid;
+    else hi = mid;
   }
-  // Block antenna span (from its first and last threads' points).
-  if (threadIdx.x == 0) s_a0 = a;
+  *owned = A > 0 && offsets[lo] <= pi && pi < offsets[lo + 1];
+  return lo;
+}
+
+// Gradients of one live (uncut, in-bounds) point pi of antenna a.  The residual
+// row comes from shared memory (rr, ri: ld floats each) or, when rr is null,
+// from global memory.
+template <typename T, bool WITH_POINTS>
+__device__ __forceinline__ void ragged_point_grads(const RgP<T>& p, int64_t pi, int64_t a, const float* rr,
+                                                   const float* ri, int ld) {
+  float nrm[3], pt[3], txp[3], rxp[3];
+  ld3(p.normals, pi, nrm);
+  ld3(p.points, pi, pt);
+  ld3(p.tx, a, txp);
+  ld3(p.rx, a, rxp);
+  SpecGeom geo;
+  specular_geometry(txp, rxp, nrm, pt, geo);
+  const double px = pt[0], py = pt[1], pz = pt[2];
+  const PhaseCycles pc = path_cycles(txp[0] - px, txp[1] - py, txp[2] - pz, rxp[0] - px, rxp[1] - py,
+                                     rxp[2] - pz, p.k0, p.b0, p.k1, p.b1);
+  const float2 zt = cis_cycles(pc.dcyc);
+  float qr = 0.0f, qi = 0.0f, dr = 0.0f, di = 0.0f;
+  auto step = [&](float cr, float ci) {
+    if (WITH_POINTS) {
+      const float ndr = fmaf(dr, zt.x, fmaf(-di, zt.y, qr));
+      const float ndi = fmaf(dr, zt.y, fmaf(di, zt.x, qi));
+      dr = ndr;
+      di = ndi;
+    }
+    const float nqr = fmaf(qr, zt.x, fmaf(-qi, zt.y, cr));
+    const float nqi = fmaf(qr, zt.y, fmaf(qi, zt.x, -ci));
+    qr = nqr;
+    qi = nqi;
+  };
+  if (rr != nullptr) {
+    for (int n = ld - 4; n >= 0; n -= 4) {
+      const float4 x = lds4(rr + n);
+      const float4 y = lds4(ri + n);
+      step(x.w, y.w);
+      step(x.z, y.z);
+      step(x.y, y.y);
+      step(x.x, y.x);
+    }
+  } else {
+    for (int64_t n = p.S - 1; n >= 0; --n) step(ld_f(p.gr, a * p.S + n), ld_f(p.gi, a * p.S + n));
+  }
+  const float inv_pa = 1.0f / static_cast<float>(p.offsets[a + 1] - p.offsets[a]);
+  const float2 e0 = cis_cycles(pc.frac0);
+  const float sum_re = cmul(e0, make_float2(qr, qi)).x;
+  const float propagation_distance = path_distance(txp, rxp, pt);
+  const float atten = 1.0f / sq(propagation_distance);
+  const float sigma_value = ld_f(p.sigmas, pi);
+  p.g_sigmas[pi] = from_f<T>(atten * geo.align * sum_re * inv_pa);
+  float gsa[3];
+  align_normal_gradient(geo, nrm, gsa);
+  const float normal_scale = sigma_value * atten;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) p.g_normals[pi * 3 + k] = from_f<T>(normal_scale * gsa[k] * sum_re * inv_pa);
+  if (WITH_POINTS) {
+    const float w0 = static_cast<float>(2.0 * static_cast<double>(kPiF) * p.f0);
+    const float w1s = static_cast<float>(2.0 * static_cast<double>(kPiF) * p.As / p.fs);
+    const float2 q1 = cmul(zt, make_float2(dr, di));
+    const float2 f = cmul(e0, make_float2(w0 * qr + w1s * q1.x, w0 * qi + w1s * q1.y));
+    const float amp = sigma_value * geo.align * atten;
+    const float d_tau = -amp * f.y;
+    const float dist_t = sqrtf(sq(txp[0] - pt[0]) + sq(txp[1] - pt[1]) + sq(txp[2] - pt[2]));
+    const float dist_r = sqrtf(sq(rxp[0] - pt[0]) + sq(rxp[1] - pt[1]) + sq(rxp[2] - pt[2]));
+    float drho[3];
+    align_point_gradient(geo, nrm, dist_t, dist_r, drho);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float dD = geo.inc[k] - geo.ret[k];
+      const float damp_dp = normal_scale * drho[k] - 2.0f * amp / propagation_distance * dD;
+      p.g_points[pi * 3 + k] = from_f<T>((sum_re * damp_dp + d_tau * dD / kSpeedOfLight) * inv_pa);
+    }
+  }
+}
+
+// Adjoint.  A block screens kBwdTile consecutive points, kBwdCand per thread:
+// it finds each point's antenna, culls it by the specular geometry, and writes
+// zero gradients for culled, out-of-bounds and unowned points; the live points
+// are listed in shared memory and then dealt out over the block, so every lane
+// runs the full sample recurrence of a live point.  (About 60% of a typical
+// step's points are live; with one point per thread 40% of the lanes would sit
+// out the recurrence.)  A point's gradients depend on that point only, so the
+// results do not depend on the list order.  Residual rows of the antennas the
+// tile spans are staged in shared memory when there are few of them (points
+// are grouped by antenna, so a tile usually lies within one antenna).
+constexpr int kBwdThreads = 128;
+constexpr int kBwdCand = 8;
+constexpr int kBwdTile = kBwdThreads * kBwdCand;
+
+template <typename T, bool WITH_POINTS>
+__global__ void __launch_bounds__(kBwdThreads) ragged_bwd_kernel(const RgP<T> p, int ld, int max_rows) {
+  extern __shared__ __align__(16) float srow[];  // [max_rows][2][ld]
+  __shared__ int s_live[kBwdTile];
+  __shared__ int s_nlive;
+  __shared__ long long s_a0, s_a1;
+  const int64_t base = blockIdx.x * static_cast<int64_t>(kBwdTile);
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    bool owned;
+    s_nlive = 0;
+    s_a0 = point_antenna(p.offsets, p.A, base, &owned);
+    s_a1 = point_antenna(p.offsets, p.A, min(p.P, base + kBwdTile) - 1, &owned);
+  }
   __syncthreads();
-  if (inside && (threadIdx.x == blockDim.x - 1 || pi == p.P - 1)) s_a1 = a;
-  __syncthreads();
+  for (int k = 0; k < kBwdCand; ++k) {
+    const int c = threadIdx.x + k * kBwdThreads;
+    const int64_t pi = base + c;
+    bool live = false;
+    if (pi < p.P) {
+      bool owned;
+      const int64_t a = point_antenna(p.offsets, p.A, pi, &owned);
+      if (!owned && p.status != nullptr) atomicExch(p.status, kStatusBadOffsets);
+      if (owned && (p.inb == nullptr || p.inb[pi])) {
+        float nrm[3], pt[3], txp[3], rxp[3];
+        ld3(p.normals, pi, nrm);
+        ld3(p.points, pi, pt);
+        ld3(p.tx, a, txp);
+        ld3(p.rx, a, rxp);
+        SpecGeom geo;
+        specular_geometry(txp, rxp, nrm, pt, geo);
+        live = !culled(geo);
+      }
+      if (!live) {
+        p.g_sigmas[pi] = from_f<T>(0.0f);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) p.g_normals[pi * 3 + q] = from_f<T>(0.0f);
+        if (WITH_POINTS) {
+#pragma unroll
+          for (int q = 0; q < 3; ++q) p.g_points[pi * 3 + q] = from_f<T>(0.0f);
+        }
+      }
+    }
+    const unsigned ballot = __ballot_sync(0xffffffffu, live);
+    if (ballot != 0u) {
+      int wbase = 0;
+      if (lane == 0) wbase = atomicAdd(&s_nlive, __popc(ballot));
+      wbase = __shfl_sync(0xffffffffu, wbase, 0);
+      if (live) s_live[wbase + __popc(ballot & ((1u << lane) - 1u))] = c;
+    }
+  }
   const int64_t a0 = s_a0;
   const int64_t a1 = max(s_a0, s_a1);
   const bool staged = p.A > 0 && (a1 - a0 + 1) <= max_rows;
   if (staged) {
     const int rows = static_cast<int>(a1 - a0 + 1);
-    for (int i = threadIdx.x; i < rows * ld; i += blockDim.x) {
+    for (int i = threadIdx.x; i < rows * ld; i += kBwdThreads) {
       const int r = i / ld, c = i - r * ld;
       float vr = 0.0f, vi = 0.0f;
       if (c < p.S) {
@@ -322,89 +448,16 @@ __global__ void __launch_bounds__(128) ragged_bwd_kernel(const RgP<T> p, int ld,
     }
   }
   __syncthreads();
-  if (!inside) return;
-
-  float gn[3] = {0.0f, 0.0f, 0.0f}, gp[3] = {0.0f, 0.0f, 0.0f};
-  float gsig = 0.0f;
-  const bool active = owned && (p.inb == nullptr || p.inb[pi]);
-  if (active) {
-    float nrm[3], pt[3], txp[3], rxp[3];
-    ld3(p.normals, pi, nrm);
-    ld3(p.points, pi, pt);
-    ld3(p.tx, a, txp);
-    ld3(p.rx, a, rxp);
-    SpecGeom geo;
-    specular_geometry(txp, rxp, nrm, pt, geo);
-    if (!culled(geo)) {
-      const double px = pt[0], py = pt[1], pz = pt[2];
-      const PhaseCycles pc = path_cycles(txp[0] - px, txp[1] - py, txp[2] - pz, rxp[0] - px,
-                                         rxp[1] - py, rxp[2] - pz, p.k0, p.b0, p.k1, p.b1);
-      const float2 zt = cis_cycles(pc.dcyc);
-      float qr = 0.0f, qi = 0.0f, dr = 0.0f, di = 0.0f;
-      auto step = [&](float cr, float ci) {
-        if (WITH_POINTS) {
-          const float ndr = fmaf(dr, zt.x, fmaf(-di, zt.y, qr));
-          const float ndi = fmaf(dr, zt.y, fmaf(di, zt.x, qi));
-          dr = ndr;
-          di = ndi;
-        }
-        const float nqr = fmaf(qr, zt.x, fmaf(-qi, zt.y, cr));
-        const float nqi = fmaf(qr, zt.y, fmaf(qi, zt.x, -ci));
-        qr = nqr;
-        qi = nqi;
-      };
-      if (staged) {
-        const float* rr = srow + ((a - a0) * 2 + 0) * ld;
-        const float* ri = srow + ((a - a0) * 2 + 1) * ld;
-        for (int n = ld - 4; n >= 0; n -= 4) {
-          const float4 x = lds4(rr + n);
-          const float4 y = lds4(ri + n);
-          step(x.w, y.w);
-          step(x.z, y.z);
-          step(x.y, y.y);
-          step(x.x, y.x);
-        }
-      } else {
-        for (int64_t n = p.S - 1; n >= 0; --n) step(ld_f(p.gr, a * p.S + n), ld_f(p.gi, a * p.S + n));
-      }
-      const float inv_pa = 1.0f / static_cast<float>(p.offsets[a + 1] - p.offsets[a]);
-      const float2 e0 = cis_cycles(pc.frac0);
-      const float sum_re = cmul(e0, make_float2(qr, qi)).x;
-      const float propagation_distance = path_distance(txp, rxp, pt);
-      const float atten = 1.0f / sq(propagation_distance);
-      const float sigma_value = ld_f(p.sigmas, pi);
-      gsig = atten * geo.align * sum_re * inv_pa;
-      float gsa[3];
-      align_normal_gradient(geo, nrm, gsa);
-      const float normal_scale = sigma_value * atten;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) gn[k] = normal_scale * gsa[k] * sum_re * inv_pa;
-      if (WITH_POINTS) {
-        const float w0 = static_cast<float>(2.0 * static_cast<double>(kPiF) * p.f0);
-        const float w1s = static_cast<float>(2.0 * static_cast<double>(kPiF) * p.As / p.fs);
-        const float2 q1 = cmul(zt, make_float2(dr, di));
-        const float2 f = cmul(e0, make_float2(w0 * qr + w1s * q1.x, w0 * qi + w1s * q1.y));
-        const float amp = sigma_value * geo.align * atten;
-        const float d_tau = -amp * f.y;
-        const float dist_t = sqrtf(sq(txp[0] - pt[0]) + sq(txp[1] - pt[1]) + sq(txp[2] - pt[2]));
-        const float dist_r = sqrtf(sq(rxp[0] - pt[0]) + sq(rxp[1] - pt[1]) + sq(rxp[2] - pt[2]));
-        float drho[3];
-        align_point_gradient(geo, nrm, dist_t, dist_r, drho);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const float dD = geo.inc[k] - geo.ret[k];
-          const float damp_dp = normal_scale * drho[k] - 2.0f * amp / propagation_distance * dD;
-          gp[k] = (sum_re * damp_dp + d_tau * dD / kSpeedOfLight) * inv_pa;
-        }
-      }
-    }
-  }
-  p.g_sigmas[pi] = from_f<T>(gsig);
-#pragma unroll
-  for (int k = 0; k < 3; ++k) p.g_normals[pi * 3 + k] = from_f<T>(gn[k]);
-  if (WITH_POINTS) {
-#pragma unroll
-    for (int k = 0; k < 3; ++k) p.g_points[pi * 3 + k] = from_f<T>(gp[k]);
+  const int nlive = s_nlive;
+  for (int i = threadIdx.x; i < nlive; i += kBwdThreads) {
+    const int64_t pi = base + s_live[i];
+    bool owned;
+    const int64_t a = point_antenna(p.offsets, p.A, pi, &owned);
+    // A row outside the staged span (possible only with non-monotonic offsets) is read from global memory.
+    const bool row_staged = staged && a >= a0 && a <= a1;
+    const float* rr = row_staged ? srow + ((a - a0) * 2 + 0) * ld : nullptr;
+    const float* ri = row_staged ? srow + ((a - a0) * 2 + 1) * ld : nullptr;
+    ragged_point_grads<T, WITH_POINTS>(p, pi, a, rr, ri, ld);
   }
 }
 
@@ -521,9 +574,10 @@ cudaError_t launch_ragged_bwd(const RaggedArgs& a, cudaStream_t st) {
                                : reinterpret_cast<const void*>(&ragged_bwd_kernel<T, false>);
   cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (err != cudaSuccess) return err;
-  const int64_t blocks = (a.P + 127) / 128;
+  const int64_t blocks = (a.P + kBwdTile - 1) / kBwdTile;
+  if (blocks > 0x7fffffff) return cudaErrorInvalidConfiguration;
   void* args[] = {&p, const_cast<int*>(&ld), const_cast<int*>(&max_rows)};
-  return cudaLaunchKernel(fn, dim3(static_cast<unsigned>(blocks)), dim3(128), args, smem, st);
+  return cudaLaunchKernel(fn, dim3(static_cast<unsigned>(blocks)), dim3(kBwdThreads), args, smem, st);
 }
 
 }  // namespace
