@@ -247,6 +247,23 @@ struct SpreadP {
   double k0, b0, k1, b1;
 };
 
+struct SpreadVoxel {
+  float x, y, z, gr, gi;
+};
+
+template <typename T>
+__device__ __forceinline__ SpreadVoxel load_spread_voxel(const SpreadP<T>& p, int64_t v, int64_t v_end) {
+  SpreadVoxel s{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  if (v < v_end) {
+    s.x = ld_f(p.voxel, v);
+    s.y = ld_f(p.voxel, p.N + v);
+    s.z = ld_f(p.voxel, 2 * p.N + v);
+    s.gr = ld_f(p.gr, v);
+    s.gi = ld_f(p.gi, v);
+  }
+  return s;
+}
+
 template <typename T, int W>
 __global__ void __launch_bounds__(kSpreadThreads) nufft_spread_kernel(const SpreadP<T> p) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -297,12 +314,17 @@ __global__ void __launch_bounds__(kSpreadThreads) nufft_spread_kernel(const Spre
   const int64_t v_end = min(p.N, v_begin + p.vox_per_split);
   float* col_re = buf + threadIdx.x;             // window column of this thread
   float* col_im = buf + kWin * kWinLd + threadIdx.x;
+  // The next voxel's inputs are loaded while the current one is spread (the
+  // shared windows leave room for few warps to hide the load latency).
+  SpreadVoxel next = load_spread_voxel(p, v_begin + threadIdx.x, v_end);
   for (int64_t v = v_begin + threadIdx.x; v < v_end; v += blockDim.x) {
-    const double x = static_cast<double>(ld_f(p.voxel, v));
-    const double y = static_cast<double>(ld_f(p.voxel, p.N + v));
-    const double z = static_cast<double>(ld_f(p.voxel, 2 * p.N + v));
-    const float g_r = ld_f(p.gr, v);
-    const float g_i = ld_f(p.gi, v);
+    const SpreadVoxel cur = next;
+    next = load_spread_voxel(p, v + blockDim.x, v_end);
+    const double x = static_cast<double>(cur.x);
+    const double y = static_cast<double>(cur.y);
+    const double z = static_cast<double>(cur.z);
+    const float g_r = cur.gr;
+    const float g_i = cur.gi;
     const NufftPoint q = nufft_point<W>(pos[0], pos[1], pos[2], pos[3], pos[4], pos[5], x, y, z, p.k0,
                                         p.b0, p.k1, p.b1, p.h, fM);
     const float2 e = cis_cycles(q.frac);

@@ -51,6 +51,28 @@ struct TrSpreadP {
   double k0, b0, k1, b1;
 };
 
+struct SpreadPoint {
+  float nx, ny, nz, px, py, pz, sig;
+  bool inb;
+};
+
+template <typename T>
+__device__ __forceinline__ SpreadPoint load_spread_point(const TrSpreadP<T>& p, int64_t a, int64_t q,
+                                                         int64_t p_end) {
+  SpreadPoint s{0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, false};
+  s.inb = q < p_end && p.inb[q];
+  if (s.inb) {
+    s.nx = ld_f(p.normals, q * 3 + 0);
+    s.ny = ld_f(p.normals, q * 3 + 1);
+    s.nz = ld_f(p.normals, q * 3 + 2);
+    s.px = ld_f(p.points, q * 3 + 0);
+    s.py = ld_f(p.points, q * 3 + 1);
+    s.pz = ld_f(p.points, q * 3 + 2);
+    s.sig = ld_f(p.sigmas, a * p.P + q);
+  }
+  return s;
+}
+
 template <typename T, int W>
 __global__ void __launch_bounds__(kSpreadThreads) nufft_tracer_spread_kernel(const TrSpreadP<T> p) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -103,19 +125,20 @@ __global__ void __launch_bounds__(kSpreadThreads) nufft_tracer_spread_kernel(con
   const int64_t p_end = min(p.P, p_begin + p.pts_per_split);
   float* col_re = buf + threadIdx.x;
   float* col_im = buf + kWin * kWinLd + threadIdx.x;
+  // The next point's inputs are loaded while the current one is spread (the
+  // shared windows leave room for few warps to hide the load latency).
+  SpreadPoint next = load_spread_point(p, a, p_begin + threadIdx.x, p_end);
   for (int64_t q = p_begin + threadIdx.x; q < p_end; q += blockDim.x) {
-    if (!p.inb[q]) continue;
-    float nrm[3], pt[3];
-    nrm[0] = ld_f(p.normals, q * 3 + 0);
-    nrm[1] = ld_f(p.normals, q * 3 + 1);
-    nrm[2] = ld_f(p.normals, q * 3 + 2);
-    pt[0] = ld_f(p.points, q * 3 + 0);
-    pt[1] = ld_f(p.points, q * 3 + 1);
-    pt[2] = ld_f(p.points, q * 3 + 2);
+    const SpreadPoint cur = next;
+    next = load_spread_point(p, a, q + blockDim.x, p_end);
+    if (!cur.inb) continue;
+    const float nrm[3] = {cur.nx, cur.ny, cur.nz};
+    const float pt[3] = {cur.px, cur.py, cur.pz};
+    const float sig = cur.sig;
     SpecGeom geo;
     specular_geometry(txp, rxp, nrm, pt, geo);
     if (culled(geo)) continue;
-    const float amp = ld_f(p.sigmas, a * p.P + q) * geo.align / sq(path_distance(txp, rxp, pt));
+    const float amp = sig * geo.align / sq(path_distance(txp, rxp, pt));
     const NufftPoint np = nufft_point<W>(pos[0], pos[1], pos[2], pos[3], pos[4], pos[5],
                                          static_cast<double>(pt[0]), static_cast<double>(pt[1]),
                                          static_cast<double>(pt[2]), p.k0, p.b0, p.k1, p.b1, p.h, fM);
