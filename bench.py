@@ -15,14 +15,17 @@ inside the timed region.  Under torchrun each rank backprojects its own 128^3
 slab of a taller volume (weak scaling, no collective on the data path).
 
 Also reported: the FP32-pipe roofline of the kernel (algorithmic 8 flops per
-voxel-antenna-sample over the measured FP32 FMA rate), the PLAIN form on a
-voxel subset, the MF adjoint, the tracer forward + adjoint in rays/s, relative
-L2 errors against the FP64 oracle, clocks during the timed region, and the CPU
-baseline (the reference-order FP32 oracle port on the host cores).
+voxel-antenna-sample over the measured FP32 FMA rate) with the measured ceiling
+of its Horner loop, and clocks during the timed region.  At N = 1 the line adds
+the extras: the PLAIN forward and adjoint, the MIXED MF adjoint, the NUFFT form,
+the tracer forward + adjoint in rays/s, the ragged and stage-1 steps, relative
+L2 errors against the FP64 oracle, and the CPU baseline (the reference-order
+FP32 oracle port on the host cores).
 
 ``--impl reference`` times the reference's CPU path -- here the FP32
-reference-order restatement in oracle/ (the reference has no CPU code; its CUDA
-kernels are the GPU parity pin) -- on a bounded voxel sample of the same workload.
+reference-order restatement in oracle/ (the reference has no CPU code) -- on a
+bounded voxel sample of the same workload, and adds the reference's own CUDA
+kernels (rebuilt for sm_100a into oracle/_ref) timed on this GPU.
 """
 from __future__ import annotations
 
@@ -392,10 +395,12 @@ def run_ours(args):
             "kernel_frac_of_ceiling": round(achieved / ceiling, 4),
             "source": "geraf_rf_horner_probe (the forward's packed Horner loop alone) in this process"}
 
-    wanted = set() if args.no_extras else {x.strip() for x in args.extras.split(",") if x.strip()}
+    # The extras are single-GPU measurements: under torchrun (N > 1) they would only hold
+    # every GPU while rank 0 repeats them, so they run at N = 1 alone.
+    wanted = set() if args.no_extras or world > 1 else {x.strip() for x in args.extras.split(",") if x.strip()}
     if rank == 0 and wanted:
         line.update(extras(args, wl, dev, out_r, out_i, wanted))
-        if world == 1 and "cpu" in wanted:
+        if "cpu" in wanted:
             line["cpu_baseline"], line["rel_err_vs_fp64"] = cpu_leg(wl, out_r, out_i, dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
