@@ -1027,14 +1027,38 @@ cudaError_t launch_tracer_bwd_finalize(int dtype, const float* partial, int spli
   return cudaGetLastError();
 }
 
+// Resident blocks per SM of the MIXED forward at this shape, from the occupancy
+// calculator; the thread-count bound when no device answers.
+int tr_fwd_blocks_per_sm(const TracerArgs& a, const Tuning& t, int groups) {
+  const bool f64 = a.dtype == kF64;
+  const void* fn = t.chunk == 8    ? (f64 ? reinterpret_cast<const void*>(&tracer_fwd_mixed_kernel<double, 8>)
+                                          : reinterpret_cast<const void*>(&tracer_fwd_mixed_kernel<float, 8>))
+                   : t.chunk == 32 ? (f64 ? reinterpret_cast<const void*>(&tracer_fwd_mixed_kernel<double, 32>)
+                                          : reinterpret_cast<const void*>(&tracer_fwd_mixed_kernel<float, 32>))
+                                   : (f64 ? reinterpret_cast<const void*>(&tracer_fwd_mixed_kernel<double, 16>)
+                                          : reinterpret_cast<const void*>(&tracer_fwd_mixed_kernel<float, 16>));
+  const size_t smem = fwd_mixed_smem(t.threads, groups, t.chunk);
+  int n = 0;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, t.threads, smem) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return std::max(1, 512 / t.threads);
+  }
+  return n;
+}
+
 Tuning tracer_forward_resolve(const TracerArgs& a, const Tuning& req) {
   if (a.mode == kNufft) return tracer_nufft_forward_resolve(a, req);
   Tuning t = req;
-  // MIXED: 64-thread blocks (measured on B200 for 64 antennas x 524288 points x 128
-  // samples: 0.66 ms against 0.84 ms with 256 threads -- the per-tile compaction
-  // barriers stall fewer warps, and more blocks fit each SM).
+  // MIXED: 64-thread blocks of 8-sample chunks (measured on B200 for 64 antennas x
+  // 524288 points x 128 samples: 0.56 ms, against 0.70 ms with 16-sample chunks and
+  // 0.84 ms with 256 threads; 128 antennas x 262144 points x 256 samples: 0.69 ms
+  // against 0.76 ms).  Small blocks stall fewer warps at the per-tile compaction
+  // barriers, and short chunks hold fewer accumulators, so more blocks fit each SM
+  // to hide the latency of the per-point geometry.
   if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = a.mode == kMixed ? 64 : 256;
-  if (t.chunk != 8 && t.chunk != 16 && t.chunk != 32) t.chunk = 16;
+  if (t.chunk != 8 && t.chunk != 16 && t.chunk != 32) t.chunk = a.mode == kMixed ? 8 : 16;
   if (t.items <= 0) t.items = 1;
   if (t.stage_rows <= 0) t.stage_rows = 8;
   if (a.mode == kPlain) {
@@ -1047,8 +1071,8 @@ Tuning tracer_forward_resolve(const TracerArgs& a, const Tuning& req) {
   const int64_t ptiles = std::max<int64_t>(1, (a.P + t.threads - 1) / t.threads);
   if (t.splits <= 0) {
     const DeviceInfo dev = current_device_info();
-    const int per_sm = std::max(1, 512 / t.threads);
-    t.splits = pick_splits(std::max<int64_t>(1, a.A * ranges), per_sm, dev.sm_count, ptiles);
+    t.splits = pick_splits(std::max<int64_t>(1, a.A * ranges), tr_fwd_blocks_per_sm(a, t, groups),
+                           dev.sm_count, ptiles);
   }
   t.splits = static_cast<int>(std::min<int64_t>(std::max(t.splits, 1), ptiles));
   return t;
