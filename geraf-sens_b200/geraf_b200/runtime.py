@@ -34,7 +34,7 @@ def default_precision() -> str:
     """Arithmetic form used when a call does not name one.
 
     ``mixed`` (FP64 phase reduction, Horner / rotator phasors, compensated
-    sums; judged against an FP64 oracle) unless ``GERAF_RF_PRECISION`` names
+    sums; checked against an FP64 oracle) unless ``GERAF_RF_PRECISION`` names
     ``plain`` (the reference's FP32 arithmetic, expression for expression) or
     ``nufft`` (the fast approximate form of the matched filter and the signal
     tracer: MIXED phases, the sample sums through oversampled range FFTs and a

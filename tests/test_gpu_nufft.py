@@ -101,7 +101,7 @@ def test_odd_and_small_sample_counts(cuda, S):
 def test_element_types(cuda, case, dtype, tol):
     c, ch = case, case["ch"]
     if dtype == torch.float16:
-        # judged against the oracle on the half-rounded inputs
+        # checked against the oracle on the half-rounded inputs
         c = {k: (v.astype(np.float16).astype(np.float32) if isinstance(v, np.ndarray) else v)
              for k, v in c.items()}
     ref = oracle_fwd(c)
