@@ -494,9 +494,12 @@ __global__ void __launch_bounds__(128) tracer_bwd_plain_kernel(const TrP<T> p) {
 // them out evenly over all threads: no lane idles beside a lane that works.
 // Each pair's normal / position contributions land in shared memory, and the
 // point's owner thread adds them up in antenna order -- the same sums, in the
-// same order, as one thread walking its point's antennas.
+// same order, as one thread walking its point's antennas.  Six blocks are kept
+// resident per SM (80 registers, no spills): 1-6% faster than the five that 93
+// registers allowed, measured on 64 antennas x 524288 points x 128 samples and
+// 128 antennas x 262144 points x 256 samples.
 template <typename T, bool WITH_POINTS>
-__global__ void __launch_bounds__(128) tracer_bwd_mixed_kernel(const TrP<T> p) {
+__global__ void __launch_bounds__(128, 6) tracer_bwd_mixed_kernel(const TrP<T> p) {
   constexpr int NC = WITH_POINTS ? 6 : 3;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
