@@ -187,3 +187,27 @@ def test_stage1_eval_geometry_helpers():
     a = torch.tensor(rng.standard_normal((300, 3)), dtype=torch.float32)
     assert ev.chamfer(a, a) == 0.0
     assert ev.chamfer(a, a + torch.tensor([0.01, 0.0, 0.0])) > 0.0
+
+
+def test_missing_library_fails_loudly():
+    """Without the built CUDA library the loader every operator goes through raises:
+    nothing falls back to a CPU path."""
+    import os
+    import subprocess
+    import sys
+
+    code = (
+        "import torch\n"
+        "from geraf_b200 import _lib\n"
+        "_lib.LIB_PATH = '/nonexistent/libgeraf_rf.so'\n"
+        "from geraf_b200.ops.RFMatchedFilter import _C\n"
+        "try:\n"
+        "    _lib.load()\n"
+        "except ImportError as e:\n"
+        "    print('raised:', e)\n"
+    )
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, PYTHONPATH=os.path.join(root, "geraf-sens_b200") + os.pathsep + root)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert "raised:" in out.stdout and "not found" in out.stdout
