@@ -60,6 +60,8 @@ def parse_args(argv=None):
                          "ragged, stage1, cpu")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--stage1-steps", type=int, default=160,
+                    help="training steps per form of the stage-1 equal-error comparison")
     return ap.parse_args(argv)
 
 
@@ -156,9 +158,9 @@ def fp32_peak_tflops(dev) -> float:
     """Measured FP32 FMA rate of this GPU (the roofline denominator)."""
     import torch
 
-    from geraf_b200 import _lib
+    from benchkit import probes
 
-    lib = _lib.load()
+    lib = probes.lib()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     blocks, threads, iters = sms * 8, 256, 1 << 12
     sink = torch.empty(blocks * threads, device=dev)
@@ -167,7 +169,7 @@ def fp32_peak_tflops(dev) -> float:
     for _ in range(4):
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
-        _lib.check(lib.geraf_rf_fma_probe(blocks, threads, iters, sink.data_ptr(), stream), "probe")
+        probes.check(lib.geraf_rf_fma_probe(blocks, threads, iters, sink.data_ptr(), stream), "probe")
         e.record()
         e.synchronize()
         ms = s.elapsed_time(e)
@@ -180,9 +182,9 @@ def horner_ceiling_tflops(dev) -> float:
     no per-(voxel, antenna) set-up), the ceiling of that loop's instruction form."""
     import torch
 
-    from geraf_b200 import _lib
+    from benchkit import probes
 
-    lib = _lib.load()
+    lib = probes.lib()
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     blocks, threads, rows = sms * 3, 128, 256
     sink = torch.empty(blocks * threads, device=dev)
@@ -191,7 +193,8 @@ def horner_ceiling_tflops(dev) -> float:
     for _ in range(4):
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
-        _lib.check(lib.geraf_rf_horner_probe(blocks, threads, rows, sink.data_ptr(), stream), "horner probe")
+        probes.check(lib.geraf_rf_horner_probe(blocks, threads, rows, sink.data_ptr(), stream),
+                     "horner probe")
         e.record()
         e.synchronize()
         best = max(best, blocks * threads * rows * 16384 / (s.elapsed_time(e) * 1e-3) / 1e12)
@@ -202,7 +205,7 @@ def make_mf_workload(name, rank, world, dev, seed):
     import numpy as np
     import torch
 
-    from geraf_b200 import scenes
+    from benchkit import scenes
 
     w = scenes.mf_full_workload(seed) if name == "mf-full" else scenes.mf_small_workload(seed)
     vox = w["voxel"].copy()
@@ -215,6 +218,40 @@ def make_mf_workload(name, rank, world, dev, seed):
                                   w["chirp"], snr_db=w["snr_db"], generator=gen)
     return dict(tx=tx, rx=rx, real=re, imag=im, voxel=torch.tensor(vox, device=dev), chirp=w["chirp"],
                 A=tx.shape[0], S=w["chirp"].num_samples, N=vox.shape[1], positions=w["positions"])
+
+
+def workload_config(name: str, A: int, S: int, N: int) -> dict:
+    """The workload as both arms name it (identical dicts, so the two lines
+    describe the same job); the arithmetic form and launch shape are reported
+    beside it under ``form``."""
+    return {"workload": f"{name}: {A} virtual channels x {S} ADC samples x {N} voxels per GPU",
+            "antennas": A, "samples": S, "voxels_per_gpu": N,
+            "l2": ("GPU arm: flushed between timed steps (256 MiB write); CPU arm: the host "
+                   "path has no device L2 to flush")}
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
+def spec_fp32_tflops(dev, sm_mhz: float | None) -> float | None:
+    """The FP32 FMA issue rate the SM count and a clock imply: SMs x 128 lanes x
+    2 flops x clock (the sampled median clock under load)."""
+    import torch
+
+    if not sm_mhz:
+        return None
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    return sms * 128 * 2 * sm_mhz * 1e6 / 1e12
 
 
 def mf_call(wl, out_r, out_i, precision, voxel=None, N=None, tuning=None):
@@ -367,16 +404,14 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded point-scatterer scene; reference RF data not released)",
-        "config": {
-            "workload": (f"{args.workload}: {A} virtual channels x {S} ADC samples x {N} voxels "
-                         f"per GPU ({args.precision} form)"),
-            "antennas": A, "samples": S, "voxels_per_gpu": N, "precision": args.precision,
+        "config": workload_config(args.workload, A, S, N),
+        "form": {
+            "precision": args.precision,
             "phase_reduction": "f64" if args.precision == "mixed" else "f32 (reference order)",
-            "l2": "flushed between timed steps (256 MiB write)",
-            "parallelism": f"voxel slabs x{world}, no collective",
             "launch_shape": tuned or "library default",
             "autotuned_candidates": n_cands,
         },
+        "parallelism": f"voxel slabs x{world}, no collective",
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "roofline": {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 3),
@@ -387,6 +422,11 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clock_info,
     }
+    spec = spec_fp32_tflops(dev, (clock_info or {}).get("sm_mhz"))
+    if spec is not None:
+        line["roofline"]["spec_fp32_at_clock"] = {
+            "value": round(spec, 3), "unit": "TFLOP/s", "frac": round(achieved / spec, 4),
+            "source": "SMs x 128 FP32 lanes x 2 flops x the median SM clock sampled in the timed region"}
     if ceiling is not None:
         # The Horner loop alone, without the per-(voxel, antenna) set-up: the ceiling of
         # the kernel's instruction form, below the FMA-rate peak (operand fetch).
@@ -399,9 +439,10 @@ def run_ours(args):
     # every GPU while rank 0 repeats them, so they run at N = 1 alone.
     wanted = set() if args.no_extras or world > 1 else {x.strip() for x in args.extras.split(",") if x.strip()}
     if rank == 0 and wanted:
-        line.update(extras(args, wl, dev, out_r, out_i, wanted))
+        art = {"fp32_peak": peak}  # and the outputs the extras keep for the FP64 comparison
+        line.update(extras(args, wl, dev, out_r, out_i, wanted, art))
         if "cpu" in wanted:
-            line["cpu_baseline"], line["rel_err_vs_fp64"] = cpu_leg(wl, out_r, out_i, dev)
+            line["cpu_baseline"], line["rel_err_vs_fp64"] = cpu_leg(args, wl, out_r, out_i, dev, art)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -410,17 +451,19 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def extras(args, wl, dev, out_r, out_i, wanted) -> dict:
-    """Secondary measurements: PLAIN form, MF adjoint, tracer fwd+adjoint."""
+def extras(args, wl, dev, out_r, out_i, wanted, art) -> dict:
+    """Secondary measurements: PLAIN form, MF adjoint, NUFFT form, tracer
+    fwd+adjoint, ragged and stage-1 steps.  ``art`` collects outputs for the
+    FP64 comparison of the CPU leg."""
     res = {}
     if "plain" in wanted:
         res.update(_plain_extra(wl, dev))
     if "adjoint" in wanted:
-        res.update(_adjoint_extra(wl, dev))
+        res.update(_adjoint_extra(args, wl, dev, art))
     if "nufft" in wanted:
-        res.update(_nufft_extra(wl, dev, out_r, out_i))
+        res.update(_nufft_extra(wl, dev, out_r, out_i, art))
     if "tracer" in wanted:
-        res.update(_tracer_extra(args, dev))
+        res.update(_tracer_extra(args, dev, art))
     if "ragged" in wanted:
         res.update(_ragged_extra(args, dev))
     if "stage1" in wanted:
@@ -434,7 +477,7 @@ def ragged_workload(dev, seed=0, num_antennas=256, S=256):
     import numpy as np
     import torch
 
-    from geraf_b200 import scenes
+    from benchkit import scenes
 
     rng = np.random.default_rng(seed)
     tx, rx = scenes.virtual_array(64)
@@ -463,7 +506,8 @@ def _ragged_extra(args, dev) -> dict:
     """Batched uneven tracer + matched filter step (forward and adjoint), graph-captured."""
     import torch
 
-    from geraf_b200 import autotune, scenes
+    from benchkit import scenes
+    from geraf_b200 import autotune
     from geraf_b200.step import RaggedRFStep
 
     w = ragged_workload(dev, args.seed)
@@ -483,32 +527,35 @@ def _ragged_extra(args, dev) -> dict:
 
 
 def _stage1_extra(args, dev) -> dict:
-    """End-to-end stage-1 RF training step: mixed + CUDA graph vs plain eager."""
-    import torch
-
-    from geraf_b200 import autotune, scenes
-    from geraf_b200.step import Stage1RFStep
+    """End-to-end stage-1 RF training step (the reference's loss shape): its forms'
+    step times, then the equal-error comparison of MIXED + graph against PLAIN
+    eager (benchkit.stage1_eval: both train from the same initialisation on the
+    shell + torus target; Chamfer distance to the analytic surfaces at checkpoints)."""
+    from benchkit import stage1_eval
+    from benchkit.stage1 import Stage1RFStep
+    from geraf_b200 import autotune
 
     res = {}
-    vox = torch.tensor(scenes.voxel_grid(128, size=0.32).T.copy(), device=dev)
-    target = torch.ones(vox.shape[0], device=dev)
     for name, prec, mf_prec, bank, graph, iters in (("mixed_graph", "mixed", "mixed", 1, True, 5),
                                                     ("mixed_nufft_mf_graph", "mixed", "nufft", 1, True, 5),
                                                     ("nufft_graph", "nufft", "nufft", 1, True, 5),
                                                     ("mixed_bank2_graph", "mixed", "mixed", 2, True, 5),
-                                                    ("plain_eager", "plain", "plain", 1, False, 1)):
-        st = Stage1RFStep(num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=256, voxels=vox,
-                          target_mag=target, precision=prec, device=dev, seed=args.seed, mf_precision=mf_prec,
-                          bank_size=bank)
+                                                    ("plain_eager", "plain", "plain", 1, False, 2)):
+        st = Stage1RFStep(num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=256, precision=prec,
+                          device=dev, seed=args.seed, mf_precision=mf_prec, bank_size=bank)
         if graph:
             st.capture()
         ms = autotune.time_call(st.run, iters=iters, warmup=1)
         res[name] = {"ms": round(ms, 2), "it_per_s": round(1e3 / ms, 2)}
-    return {"stage1_step": {"workload": ("128 antennas x 2048 rays x 128 samples, S=256, random-init "
-                                         "SDF MLP, MF onto 128^3 voxels, L1 on |volume| + eikonal, Adam; "
-                                         "bank2: the reference's 2-chunk antenna bank, one chunk rendered "
-                                         "per step, the bank kept on the GPU"),
-                            **res}}
+    eq = stage1_eval.compare(steps=args.stage1_steps, seed=args.seed, checkpoints=4)
+    for form in ("mixed_graph", "plain_eager"):
+        eq[form].pop("loss_every_10", None)
+    return {"stage1_step": {"workload": ("128 antennas x 2048 rays x 128 target samples (64 coarse), S=256, "
+                                         "random-init SDF MLP (FP16 autocast), resample -> tracer -> MF at "
+                                         "the target points, charbonier loss + eikonal, Adam; bank2: the "
+                                         "reference's 2-chunk antenna bank, one chunk rendered per step, the "
+                                         "bank kept on the GPU"),
+                            **res, "equal_error": eq}}
 
 
 def antenna_subset(wl, a_sub):
@@ -560,33 +607,49 @@ def _plain_extra(wl, dev) -> dict:
     return res
 
 
-def _adjoint_extra(wl, dev) -> dict:
+def _adjoint_extra(args, wl, dev, art) -> dict:
+    """MIXED MF adjoint on the full workload, with its launch shape autotuned
+    first (every antenna x sample row block, a leading eighth of the voxels, so
+    the grid is the full call's)."""
     import torch
 
-    from geraf_b200 import autotune
+    from geraf_b200 import _lib, autotune
     from geraf_b200.ops.RFMatchedFilter import _C as mfc
 
     res = {}
     A, S, N = wl["A"], wl["S"], wl["N"]
     ch = wl["chirp"]
-    # MF adjoint (mixed) on the full workload
-    g_r = torch.randn(N, device=dev)
-    g_i = torch.randn(N, device=dev)
+    gen = torch.Generator(device=dev).manual_seed(args.seed + 5)
+    g_r = torch.randn(N, device=dev, generator=gen)
+    g_i = torch.randn(N, device=dev, generator=gen)
     h_r = torch.empty((A, S), device=dev)
     h_i = torch.empty((A, S), device=dev)
 
-    def adj():
-        mfc.MatchedFilter_backward_realimag(g_r, g_i, wl["real"], wl["imag"], wl["tx"], wl["rx"], h_r,
-                                            h_i, wl["voxel"], A, S, ch.adc_sample_rate, ch.As_sci, N,
-                                            precision="mixed")
+    def adj(n=N, tuning=None):
+        mfc.MatchedFilter_backward_realimag(g_r[:n], g_i[:n], wl["real"], wl["imag"], wl["tx"], wl["rx"], h_r,
+                                            h_i, wl["voxel"][:, :n].contiguous() if n < N else wl["voxel"],
+                                            A, S, ch.adc_sample_rate, ch.As_sci, n, precision="mixed",
+                                            tuning=tuning)
 
+    shape, n_cands = "library default", 0
+    if not args.no_tune:
+        n_sub = max(1, N // 8)
+        default_ms = autotune.time_call(lambda: adj(n_sub), iters=1, warmup=1)
+        best, results = autotune.tune("mf_backward", (A, S, N), _lib.MODE_MIXED,
+                                      lambda t: adj(n_sub, t), autotune.sample_major_candidates(), iters=1)
+        shape, n_cands = best, len(results)
+        gain = default_ms / min(ms for _, ms in results)
     ms = autotune.time_call(adj, iters=1, warmup=1)
     res["mf_adjoint"] = {"value": round(float(A) * S * N / (ms * 1e-3) / 1e9, 3), "unit": UNIT,
-                         "ms": round(ms, 2), "precision": "mixed"}
+                         "ms": round(ms, 2), "precision": "mixed", "launch_shape": shape,
+                         "autotuned_candidates": n_cands}
+    if n_cands:
+        res["mf_adjoint"]["tuned_speedup_vs_default"] = round(gain, 4)
+    art["mf_adjoint"] = (torch.complex(g_r, g_i).cpu().numpy(), torch.complex(h_r, h_i).cpu().numpy())
     return res
 
 
-def _nufft_extra(wl, dev, out_r, out_i) -> dict:
+def _nufft_extra(wl, dev, out_r, out_i, art) -> dict:
     """The matched filter's fast approximate form (oversampled range FFT + 8-point
     ES interpolation) on the full workload: forward and adjoint times, in the
     headline's unit (the same voxel x antenna x sample sums, evaluated in O(W)
@@ -617,7 +680,9 @@ def _nufft_extra(wl, dev, out_r, out_i) -> dict:
         mfc.MatchedFilter_backward_realimag(g_r, g_i, wl["real"], wl["imag"], wl["tx"], wl["rx"], hr, hi,
                                             wl["voxel"], A, S, ch.adc_sample_rate, ch.As_sci, N, precision=prec)
 
+    art["mf_forward_nufft"] = torch.complex(yr, yi).cpu().numpy()
     ms_b = autotune.time_call(lambda: adj("nufft", h_r, h_i), iters=2, warmup=1)
+    art["mf_adjoint_nufft"] = (torch.complex(g_r, g_i).cpu().numpy(), torch.complex(h_r, h_i).cpu().numpy())
     adj("mixed", m_r, m_i)
     ref_b = torch.complex(m_r.double(), m_i.double())
     err_b = float((torch.complex(h_r.double(), h_i.double()) - ref_b).norm() / ref_b.norm())
@@ -626,38 +691,81 @@ def _nufft_extra(wl, dev, out_r, out_i) -> dict:
     return res
 
 
-def _tracer_extra(args, dev) -> dict:
+def tracer_live_pairs(tw, chunk: int = 8) -> int:
+    """(point, antenna) pairs of the tracer workload that survive the specular
+    culling (the reference's FP32 geometry, SignalTracer_cuda_kernel.cu:172-197,
+    restated in torch on the device): the pairs whose samples the kernels sum."""
     import torch
 
-    from geraf_b200 import autotune
+    def nrm(v):
+        return v / (v.norm(dim=-1, keepdim=True) + 1e-7)
+
+    pts, n, inb = tw["points"], tw["normals"], tw["inbounds"]
+    live = 0
+    for a0 in range(0, tw["tx"].shape[0], chunk):
+        tx = tw["tx"][a0:a0 + chunk, None, :]
+        rx = tw["rx"][a0:a0 + chunk, None, :]
+        inc = nrm(pts[None] - tx)
+        idn = (inc * n[None]).sum(-1)
+        refl = nrm(inc - 2.0 * idn[..., None] * n[None])
+        align = (nrm(rx - pts[None]) * refl).sum(-1)
+        live += int(((align >= 1e-6) & (idn <= 0.0) & inb[None]).sum())
+    return live
+
+
+def _tracer_extra(args, dev, art) -> dict:
+    """Tracer forward + adjoint (with position gradients) on the 64-antenna x
+    4096-ray x 128-sample workload of a random-init SDF network: MIXED (launch
+    shapes autotuned first), NUFFT and PLAIN, in rays/s; the roofline of the
+    MIXED pair over all (point, antenna, sample) triples and over the triples of
+    live (not culled) pairs."""
+    import torch
+
+    from benchkit.sdf import tracer_workload
+    from geraf_b200 import _lib, autotune
     from geraf_b200.ops.RFSignalTracer import _C as trc
-    from geraf_b200.sdf import tracer_workload
 
     res = {}
-    # tracer forward + adjoint: 64 antennas x 4096 rays x 128 samples, S = 128
     tw = tracer_workload(device=dev, seed=args.seed)
     At, P, St = tw["A"], tw["P"], tw["chirp"].num_samples
     cfg = tw["radar_cfg"]
     xr = torch.empty((At, St), device=dev)
     xi = torch.empty((At, St), device=dev)
-    gxr = torch.randn((At, St), device=dev)
-    gxi = torch.randn((At, St), device=dev)
+    gen = torch.Generator(device=dev).manual_seed(args.seed + 7)
+    gxr = torch.randn((At, St), device=dev, generator=gen)
+    gxi = torch.randn((At, St), device=dev, generator=gen)
     gn = torch.empty((P, 3), device=dev)
     gs = torch.empty((At, P), device=dev)
     gp = torch.empty((P, 3), device=dev)
+
+    def fwd(prec, tuning=None):
+        trc.SignalTracer_forward(tw["normals"], tw["sigmas"], tw["points"], tw["tx"], tw["rx"],
+                                 tw["inbounds"], xr, xi, St, cfg["adcSampleRate"], cfg["fc_start"],
+                                 cfg["As_sci"], At, P, precision=prec, tuning=tuning)
+
+    def bwd(prec, tuning=None):
+        trc.SignalTracer_backward_normal_sigma(gxr, gxi, tw["normals"], tw["sigmas"], tw["points"],
+                                               tw["tx"], tw["rx"], tw["inbounds"], gn, gs, St,
+                                               cfg["adcSampleRate"], cfg["fc_start"], cfg["As_sci"],
+                                               At, P, grad_points=gp if prec != "plain" else None,
+                                               precision=prec, tuning=tuning)
+
+    tuned = {}
+    if not args.no_tune:
+        for op, run, cands in (("tracer_forward", fwd, autotune.sample_major_candidates()),
+                               ("tracer_backward", bwd, autotune.tracer_backward_candidates())):
+            default_ms = autotune.time_call(lambda run=run: run("mixed"), iters=5, warmup=2)
+            best, results = autotune.tune(op, (At, St, P), _lib.MODE_MIXED,
+                                          lambda t, run=run: run("mixed", t), cands, iters=5)
+            tuned[op] = {"launch_shape": best, "candidates": len(results),
+                         "tuned_speedup_vs_default": round(default_ms / min(ms for _, ms in results), 4)}
     tr = {}
     outs = {}
     for prec in ("mixed", "nufft", "plain"):
         def step(prec=prec):
-            trc.SignalTracer_forward(tw["normals"], tw["sigmas"], tw["points"], tw["tx"], tw["rx"],
-                                     tw["inbounds"], xr, xi, St, cfg["adcSampleRate"], cfg["fc_start"],
-                                     cfg["As_sci"], At, P, precision=prec)
-            trc.SignalTracer_backward_normal_sigma(gxr, gxi, tw["normals"], tw["sigmas"], tw["points"],
-                                                   tw["tx"], tw["rx"], tw["inbounds"], gn, gs, St,
-                                                   cfg["adcSampleRate"], cfg["fc_start"], cfg["As_sci"],
-                                                   At, P, grad_points=gp if prec != "plain" else None,
-                                                   precision=prec)
-        ms = autotune.time_call(step, iters=3 if prec != "plain" else 1, warmup=1)
+            fwd(prec)
+            bwd(prec)
+        ms = autotune.time_call(step, iters=5 if prec != "plain" else 1, warmup=1)
         tr[prec] = {"rays_per_s": round(At * tw["rays"] / (ms * 1e-3), 1), "ms": round(ms, 3),
                     "gpts_per_s": round(float(At) * P * St / (ms * 1e-3) / 1e9, 2)}
         outs[prec] = [torch.complex(xr, xi).to(torch.complex128)] + [t.double().clone() for t in (gs, gn, gp)]
@@ -668,19 +776,46 @@ def _tracer_extra(args, dev) -> dict:
     tr["nufft"]["rel_l2_vs_mixed"] = {k: rel(outs["nufft"][i], outs["mixed"][i])
                                       for i, k in enumerate(("signal", "grad_sigmas", "grad_normals",
                                                              "grad_points"))}
+    # roofline of the MIXED forward + adjoint: 12 flops per (point, antenna, sample)
+    live = tracer_live_pairs(tw)
+    peak = art.get("fp32_peak")
+    flops_all = 12.0 * At * P * St
+    flops_live = 12.0 * live * St
+    ms_m = tr["mixed"]["ms"]
+    roof = {"flops_per_triple": 12, "live_pair_fraction": round(live / (At * P), 4),
+            "achieved_all_tflops": round(flops_all / (ms_m * 1e-3) / 1e12, 3),
+            "achieved_live_tflops": round(flops_live / (ms_m * 1e-3) / 1e12, 3)}
+    if peak:
+        roof["peak"] = round(peak, 3)
+        roof["frac_all"] = round(flops_all / (ms_m * 1e-3) / 1e12 / peak, 4)
+        roof["frac_live"] = round(flops_live / (ms_m * 1e-3) / 1e12 / peak, 4)
+        roof["note"] = ("frac_live is the roofline: culled pairs carry no samples to sum; frac_all "
+                        "counts every triple as the reference's kernels visit them")
     res["tracer"] = {"workload": f"{At} antennas x {tw['rays']} rays x {P // tw['rays']} samples, S={St}",
                      "unit": "rays/s (ray = ray x antenna pair)", "mixed_with_point_grads": tr["mixed"],
-                     "nufft_with_point_grads": tr["nufft"], "plain": tr["plain"]}
+                     "nufft_with_point_grads": tr["nufft"], "plain": tr["plain"], "roofline": roof,
+                     "autotune": tuned or "not run"}
+    # the MIXED outputs, for the FP64 comparison in the CPU leg
+    m = outs["mixed"]
+    art["tracer"] = dict(
+        w=dict(normals=tw["normals"].cpu().numpy(), sigmas=tw["sigmas"].cpu().numpy(),
+               points=tw["points"].cpu().numpy(), tx=tw["tx"].cpu().numpy(), rx=tw["rx"].cpu().numpy(),
+               inbounds=tw["inbounds"].cpu().numpy(), S=St, fs=cfg["adcSampleRate"], f0=cfg["fc_start"],
+               As=cfg["As_sci"], rays=tw["rays"], samples_per_ray=P // tw["rays"]),
+        g=torch.complex(gxr, gxi).cpu().numpy(), x=m[0].cpu().numpy(),
+        grads={"sigmas": m[1].cpu().numpy(), "normals": m[2].cpu().numpy(), "points": m[3].cpu().numpy()})
     return res
 
 
-def cpu_leg(wl, out_r, out_i, dev):
+def cpu_leg(args, wl, out_r, out_i, dev, art):
     """CPU baseline (reference-order FP32 oracle port, all host threads) on a
-    bounded voxel sample, and FP64-oracle errors of both forms on sampled voxels."""
+    bounded voxel sample, and the FP64-oracle errors of every output the run
+    produced, on the fixed subsets of oracle/workload_parity.py."""
     import numpy as np
     import torch
 
     from oracle import rf_oracle as orc
+    from oracle import workload_parity as wp
 
     ch = wl["chirp"]
     A, S, N = wl["A"], wl["S"], wl["N"]
@@ -708,24 +843,53 @@ def cpu_leg(wl, out_r, out_i, dev):
             break
         n = int(min(16384, n * 12.0 / max(dt, 1e-3)))
     cpu = {"value": round(float(A) * S * n / dt / 1e9, 4), "unit": UNIT, "cores": orc.num_threads(),
-           "kind": "port",
-           "sample": f"{n} random voxels x {A} antennas x {S} samples ({dt:.1f} s), FP32 reference order"}
-    # errors vs FP64 on the 16 brightest voxels + 48 random ones
-    mag = torch.hypot(out_r, out_i).cpu().numpy()
-    pick = np.unique(np.concatenate([np.argsort(mag)[-16:], rng.choice(N, 48, replace=False)]))
-    fr, fi = orc.mf_forward(re, im, tx, rx, vox[:, pick], ch.adc_sample_rate, ch.As_sci, "f64")
-    ref = fr + 1j * fi
-    ours = out_r.cpu().numpy()[pick] + 1j * out_i.cpu().numpy()[pick]
-    pr = torch.empty(len(pick), device=dev)
-    pi = torch.empty(len(pick), device=dev)
-    mf_call(wl, pr, pi, "plain", voxel=wl["voxel"][:, torch.tensor(pick, device=dev)].contiguous(), N=len(pick))
-    plain = pr.cpu().numpy() + 1j * pi.cpu().numpy()
+           "kind": "port", "cpu_model": cpu_model(),
+           "sample": (f"{n} random voxels x {A} antennas x {S} samples ({dt:.1f} s), FP32 reference "
+                      f"order; extrapolated to the whole volume (the cost is linear in voxels)")}
 
-    def rel(a):
-        return float(np.linalg.norm(a - ref) / np.linalg.norm(ref))
-
-    errs = {"mf_forward_mixed": rel(ours), "mf_forward_plain": rel(plain),
-            "voxels": int(len(pick)), "how": "16 brightest + 48 random voxels vs the FP64 oracle"}
+    # ---- FP64 errors of every output (complex relative L2 on fixed subsets) ----
+    t_err = time.perf_counter()
+    w = dict(re=re, im=im, tx=tx, rx=rx, vox=vox, fs=ch.adc_sample_rate, As=ch.As_sci, S=S)
+    full = args.workload == "mf-full"
+    vi = wp.MF49152_VOXELS if full else wp.MF3072_VOXELS
+    rows = wp.MF49152_ROWS if full else wp.MF3072_ROWS
+    ref_f = wp.mf_forward_ref(w, vi)
+    ours = out_r.cpu().numpy() + 1j * out_i.cpu().numpy()
+    pr = torch.empty(len(vi), device=dev)
+    pi = torch.empty(len(vi), device=dev)
+    mf_call(wl, pr, pi, "plain", voxel=wl["voxel"][:, torch.tensor(vi, device=dev)].contiguous(), N=len(vi))
+    errs = {"mf_forward": {"mixed": wp.rel(ours[vi], ref_f),
+                           "plain": wp.rel(pr.cpu().numpy() + 1j * pi.cpu().numpy(), ref_f)}}
+    if "mf_forward_nufft" in art:
+        errs["mf_forward"]["nufft"] = wp.rel(art["mf_forward_nufft"][vi], ref_f)
+    if "mf_adjoint" in art:
+        g, h = art["mf_adjoint"]
+        ref_b = wp.mf_adjoint_ref(g, w, rows)
+        errs["mf_adjoint"] = {"mixed": wp.rel(h[rows], ref_b)}
+        if "mf_adjoint_nufft" in art and np.array_equal(art["mf_adjoint_nufft"][0], g):
+            errs["mf_adjoint"]["nufft"] = wp.rel(art["mf_adjoint_nufft"][1][rows], ref_b)
+        elif "mf_adjoint_nufft" in art:
+            g2, h2 = art["mf_adjoint_nufft"]
+            errs["mf_adjoint"]["nufft"] = wp.rel(h2[rows], wp.mf_adjoint_ref(g2, w, rows))
+    if "tracer" in art:
+        tr = art["tracer"]
+        tw = tr["w"]
+        rays = wp.fd_rays(tw)
+        pts = wp.ray_points(tw, rays)
+        adj = wp.tracer_adjoint_errors(tr["grads"], tr["g"], tw, pts)
+        errs["tracer_mixed"] = {"signal": wp.tracer_forward_error(tr["x"], tw, wp.TRACER_ROWS),
+                                "grad_sigmas": adj["sigma"], "grad_normals": adj["normal"],
+                                "grad_points": adj["position"]}
+        fd = wp.tracer_fd_errors(tr["grads"], tr["g"], tw, rays)
+        errs["tracer_mixed_vs_central_differences"] = {
+            "grad_sigmas": fd["sigma"], "grad_normals": fd["normal"], "grad_points": fd["position"],
+            "how": "largest per-ray |FD - analytic| / sum |analytic| over 256 random rays, FP64 "
+                   "central differences of the pure-torch tracer"}
+    subsets = (f"MF forward: {len(vi)} voxels ({'16^3 lattice of the 32^3 subset' if full else 'every 27th'}); "
+               f"MF adjoint: {len(rows)} antenna rows over all voxels; tracer: 16 antenna rows (signal) "
+               f"and the 32768 points of 256 random rays (gradients)")
+    errs["how"] = "complex relative L2 vs the FP64 oracle; " + subsets
+    errs["oracle_s"] = round(time.perf_counter() - t_err, 1)
     return cpu, errs
 
 
@@ -748,7 +912,7 @@ def reference_cuda_leg(args, w) -> dict:
     values) and the random-init SDF tracer scene."""
     import torch
 
-    from geraf_b200.sdf import tracer_workload
+    from benchkit.sdf import tracer_workload
     from oracle import build_ref
 
     if not torch.cuda.is_available():
@@ -846,7 +1010,7 @@ def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    from geraf_b200 import scenes
+    from benchkit import scenes
     from oracle import rf_oracle as orc
 
     w = scenes.mf_full_workload(args.seed) if args.workload == "mf-full" else scenes.mf_small_workload(args.seed)
@@ -874,16 +1038,18 @@ def run_reference(args):
     sec = float(np.mean(times))
     value = float(A) * S * n / sec / 1e9
     sample = (f"{n} random voxels of {N} x {A} antennas x {S} samples per step, "
-              f"FP32 reference-order port, {threads} threads")
+              f"FP32 reference-order port, {threads} threads; extrapolated to the whole volume "
+              f"(the cost is linear in voxels)")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded)",
-        "config": {"workload": f"{args.workload}: {A} virtual channels x {S} ADC samples x {N} voxels",
-                   "antennas": A, "samples": S, "voxels": N},
+        "config": workload_config(args.workload, A, S, N),
+        "form": {"precision": "plain", "phase_reduction": "f32 (reference order)", "host": "CPU"},
+        "parallelism": "rank 0 host threads",
         "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": sample},
+                         "cpu_model": cpu_model(), "sample": sample},
         "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     if not args.no_extras:

@@ -1,11 +1,14 @@
-// FP32 FMA issue-rate probe: the roofline denominator for the RF kernels, which
-// are bound by the FP32 pipe (no tensor-core or HBM bound applies).  No
-// counterpart in the reference.
+// Measurement probes for the benchmark and the tests (libgeraf_probe.so, not
+// part of libgeraf_rf.so): the FP32 FMA issue rate that is the roofline
+// denominator of the RF kernels (they are bound by the FP32 pipe; no
+// tensor-core or HBM bound applies), the ceiling of the MIXED forward's Horner
+// loop, and the sincosf identity check the PLAIN kernels rely on.  No
+// counterpart in the reference.  Return codes are those of geraf_rf.h.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "../../include/geraf_rf.h"
-#include "common.cuh"
+#include "../geraf-sens_b200/csrc/common.cuh"
+#include "../include/geraf_rf.h"
 
 #define GERAF_EXPORT extern "C" __attribute__((visibility("default")))
 

@@ -131,7 +131,7 @@ def synthesize_if(tx: torch.Tensor, rx: torch.Tensor, positions: torch.Tensor,
     ``positions`` [K,3], ``amplitudes`` [K] complex.  Noise power is the mean
     signal power over 10^(snr_db/10).
     """
-    from .ops.RFMatchedFilter import _C
+    from geraf_b200.ops.RFMatchedFilter import _C
 
     A, K, S = tx.shape[0], positions.shape[0], ch.num_samples
     dev = tx.device
@@ -156,16 +156,20 @@ def synthesize_if(tx: torch.Tensor, rx: torch.Tensor, positions: torch.Tensor,
 
 def synthesize_if_numpy(tx, rx, positions, amplitudes, ch: Chirp, snr_db=20.0,
                         rng: np.random.Generator | None = None):
-    """CPU (numpy, FP64) version of :func:`synthesize_if` for small cases and tests."""
+    """CPU (numpy, FP64) version of :func:`synthesize_if` for small cases and tests
+    (antennas in chunks of 256, so the [A, K, S] phase array stays small)."""
     lam_f0 = 2.0 * float(np.float32(np.pi)) * float(np.float32(MF_CARRIER))
     w1 = 2.0 * float(np.float32(np.pi)) * float(np.float32(ch.As_sci))
     t = np.arange(ch.num_samples) / float(np.float32(ch.adc_sample_rate))
-    d = (np.linalg.norm(tx[:, None, :].astype(np.float64) - positions[None], axis=-1)
-         + np.linalg.norm(rx[:, None, :].astype(np.float64) - positions[None], axis=-1)
-         + float(np.float32(0.15)))
-    tau = d / float(np.float32(C_SCALED))  # [A,K]
-    ph = tau[:, :, None] * (lam_f0 + w1 * t)[None, None, :]
-    s = (amplitudes[None, :, None] * np.exp(1j * ph)).sum(1)
+    s = np.empty((tx.shape[0], ch.num_samples), np.complex128)
+    for a0 in range(0, tx.shape[0], 256):
+        txc, rxc = tx[a0:a0 + 256], rx[a0:a0 + 256]
+        d = (np.linalg.norm(txc[:, None, :].astype(np.float64) - positions[None], axis=-1)
+             + np.linalg.norm(rxc[:, None, :].astype(np.float64) - positions[None], axis=-1)
+             + float(np.float32(0.15)))
+        tau = d / float(np.float32(C_SCALED))  # [a,K]
+        ph = tau[:, :, None] * (lam_f0 + w1 * t)[None, None, :]
+        s[a0:a0 + 256] = (amplitudes[None, :, None] * np.exp(1j * ph)).sum(1)
     if snr_db is not None:
         rng = rng or np.random.default_rng(0)
         p = np.mean(np.abs(s) ** 2)

@@ -1,0 +1,214 @@
+"""Equal-error comparison of stage-1 RF training-step forms on the shell + torus scene.
+
+The stage-1 step (:class:`benchkit.stage1.Stage1RFStep`: the reference's loss
+shape -- amplitudes at coarse samples resampled to target samples, the tracer,
+the matched filter at the target points, the "charbonier" loss against the
+target volume sampled there, the eikonal term, Adam) is trained for the same
+number of steps, from the same initialisation, rays and target, in two forms:
+
+* ``mixed`` arithmetic with the whole step captured in one CUDA graph;
+* ``plain`` arithmetic (the reference's FP32 expressions) run eagerly.
+
+The target volume is the matched-filter magnitude of the cube-shell + torus
+scene (30k point scatterers, 20 dB SNR) seen by the 49152-channel array with
+the 256-sample chirp, on a 128^3 grid over 0.32 m, mean-normalised (the
+reference divides its volumes by the transmit power).  The fixed power of the
+amplitudes is calibrated once, so the initial prediction's mean matches the
+target's; both forms use that value.
+
+At checkpoints the SDF's zero level set is extracted on a grid (sign changes
+between neighbouring grid points, linearly interpolated) and compared with
+points sampled on the analytic surfaces by the symmetric Chamfer distance; the
+network's mean |SDF| at those surface points is reported beside it.  The
+result gives the step and the time at which the MIXED form first reaches the
+PLAIN form's final Chamfer distance, so the two forms' speeds are compared at
+equal error.
+
+    python -m benchkit.stage1_eval --steps 200
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+import torch
+
+
+def analytic_surface_points(n: int, rng: np.random.Generator, cube: float = 0.3, R: float = 0.08,
+                            r: float = 0.03, center=(0.0, 0.0, 0.4)) -> np.ndarray:
+    """Area-uniform samples of the cube's outer surface and the torus surface [n, 3]."""
+    a_cube = 6 * cube * cube
+    a_torus = 4 * math.pi * math.pi * R * r
+    n_cube = int(round(n * a_cube / (a_cube + a_torus)))
+    face = rng.integers(0, 6, n_cube)
+    uv = rng.uniform(-cube / 2, cube / 2, (n_cube, 2))
+    pts = np.empty((n_cube, 3))
+    for ax in range(3):
+        m = face // 2 == ax
+        others = [o for o in range(3) if o != ax]
+        pts[m, ax] = np.where(face[m] % 2 == 0, 1.0, -1.0) * cube / 2
+        pts[m, others[0]] = uv[m, 0]
+        pts[m, others[1]] = uv[m, 1]
+    tor = []
+    n_t = n - n_cube
+    while sum(t.shape[0] for t in tor) < n_t:
+        th = rng.uniform(0, 2 * np.pi, 2 * n_t)
+        ph = rng.uniform(0, 2 * np.pi, 2 * n_t)
+        keep = rng.uniform(0, 1, 2 * n_t) < (R + r * np.cos(ph)) / (R + r)
+        th, ph = th[keep], ph[keep]
+        tor.append(np.stack([(R + r * np.cos(ph)) * np.cos(th), (R + r * np.cos(ph)) * np.sin(th),
+                             r * np.sin(ph)], 1))
+    pts = np.concatenate([pts, np.concatenate(tor, 0)[:n_t]], 0)
+    return (pts + np.asarray(center)).astype(np.float32)
+
+
+@torch.no_grad()
+def sdf_surface_points(net, center: torch.Tensor, scale: float, half: float = 0.3, res: int = 128,
+                       chunk: int = 1 << 18) -> torch.Tensor:
+    """Zero crossings of the SDF on a res^3 grid over center +- half (world coordinates)."""
+    dev = center.device
+    ax = torch.linspace(-half, half, res, device=dev)
+    gx, gy, gz = torch.meshgrid(ax, ax, ax, indexing="ij")
+    world = torch.stack([gx, gy, gz], -1).reshape(-1, 3) + center
+    vals = torch.cat([net((world[i:i + chunk] - center) / scale)[0].reshape(-1)
+                      for i in range(0, world.shape[0], chunk)]).reshape(res, res, res)
+    world = world.reshape(res, res, res, 3)
+    out = []
+    for d in range(3):
+        a = vals.narrow(d, 0, res - 1)
+        b = vals.narrow(d, 1, res - 1)
+        pa = world.narrow(d, 0, res - 1)
+        pb = world.narrow(d, 1, res - 1)
+        m = (a * b) < 0
+        t = (a[m] / (a[m] - b[m])).unsqueeze(-1)
+        out.append(pa[m] + t * (pb[m] - pa[m]))
+    return torch.cat(out, 0)
+
+
+@torch.no_grad()
+def chamfer(a: torch.Tensor, b: torch.Tensor, chunk: int = 4096) -> float:
+    """Symmetric Chamfer distance: mean nearest-neighbour distance a->b plus b->a (metres)."""
+    if a.shape[0] == 0 or b.shape[0] == 0:
+        return float("inf")
+
+    def one_way(x, y):
+        return torch.cat([torch.cdist(x[i:i + chunk], y, compute_mode="donot_use_mm_for_euclid_dist").min(1).values
+                          for i in range(0, x.shape[0], chunk)]).mean()
+
+    return float(one_way(a, b) + one_way(b, a))
+
+
+@torch.no_grad()
+def sdf_on_surface(net, center: torch.Tensor, scale: float, surface: torch.Tensor) -> float:
+    """Mean |SDF| (metres) of the network at points of the analytic surface: how far,
+    to first order, its zero level set lies from the true surface."""
+    return float((net((surface - center) / scale)[0].abs() * scale).mean())
+
+
+def target_volume(device, seed: int = 0, n: int = 128, size: float = 0.32, precision: str = "mixed"):
+    """|MF| of the shell + torus scene (49152 channels, S = 256, 20 dB SNR) on an
+    n^3 grid of ``size`` m around the scene centre, in the reference's volume
+    layout (x slowest), mean-normalised.  Returns (volume, half extent in m)."""
+    from geraf_b200.volume import build_mf_volume
+
+    from . import scenes
+    from .stage1 import SCENE_CENTER
+
+    dev = torch.device(device)
+    w = scenes.mf_full_workload(seed)
+    tx = torch.tensor(w["tx"], device=dev)
+    rx = torch.tensor(w["rx"], device=dev)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    re, im = scenes.synthesize_if(tx, rx, torch.tensor(w["positions"]), torch.tensor(w["amplitudes"]),
+                                  w["chirp"], snr_db=w["snr_db"], generator=g)
+    half = size / 2
+    c = SCENE_CENTER
+    bound = [c[0] - half, c[0] + half, c[1] - half, c[1] + half, c[2] - half, c[2] + half]
+    res = [size / (n - 1)] * 3
+    vol = build_mf_volume(re, im, tx, rx, w["chirp"].adc_sample_rate, w["chirp"].As_sci, bound, res,
+                          precision=precision, device=dev)
+    return vol / vol.mean(), half
+
+
+def train(precision: str, graph: bool, steps: int, volume, half: float, power: float, seed: int = 0,
+          checkpoints: int = 4, device="cuda", bank_size: int = 1) -> dict:
+    """Trains one form; returns its step time, losses and Chamfer distances at checkpoints."""
+    from .stage1 import SCENE_CENTER, SDF_RADIUS, Stage1RFStep
+
+    dev = torch.device(device)
+    st = Stage1RFStep(num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=256, precision=precision,
+                      device=dev, seed=seed, target_volume=volume, volume_half=half, power=power,
+                      bank_size=bank_size)
+    center = torch.tensor(SCENE_CENTER, device=dev)
+    ref = torch.tensor(analytic_surface_points(20000, np.random.default_rng(seed + 7)), device=dev)
+    curve = [(0, chamfer(sdf_surface_points(st.net, center, SDF_RADIUS), ref),
+              sdf_on_surface(st.net, center, SDF_RADIUS, ref))]
+    if graph:
+        st.capture()
+    st.gen.manual_seed(seed + 1)   # the same schedule of ray resamplings for both forms
+    every = max(1, steps // checkpoints)
+    losses = []
+    secs = 0.0
+    done = 0
+    while done < steps:
+        n = min(every, steps - done)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            st.resample()
+            losses.append(st.run().clone())
+        torch.cuda.synchronize()
+        secs += time.perf_counter() - t0
+        done += n
+        curve.append((done, chamfer(sdf_surface_points(st.net, center, SDF_RADIUS), ref),
+                      sdf_on_surface(st.net, center, SDF_RADIUS, ref)))
+    loss = torch.stack(losses).cpu().numpy()
+    return {"precision": precision, "graph": graph, "steps": steps, "ms_per_step": 1e3 * secs / steps,
+            "it_per_s": steps / secs, "loss_first": float(loss[0]), "loss_last": float(loss[-1]),
+            "loss_every_10": [float(v) for v in loss[::10]],
+            "chamfer_m": [[k, c] for k, c, _ in curve], "sdf_on_surface_m": [[k, e] for k, _, e in curve],
+            "final_chamfer_m": curve[-1][1]}
+
+
+def compare(steps: int = 200, seed: int = 0, checkpoints: int = 8) -> dict:
+    from .stage1 import Stage1RFStep
+
+    volume, half = target_volume("cuda", seed)
+    cal = Stage1RFStep(num_antennas=128, num_rays=2048, samples_per_ray=128, num_adc=256, precision="mixed",
+                       seed=seed, target_volume=volume, volume_half=half)
+    power = cal.calibrate_power()
+    del cal
+    fast = train("mixed", True, steps, volume, half, power, seed, checkpoints)
+    ref = train("plain", False, steps, volume, half, power, seed, checkpoints)
+    target = ref["final_chamfer_m"]
+    reach = next((k for k, c in fast["chamfer_m"] if k > 0 and c <= target), None)
+    out = {"workload": ("stage-1 RF step, 128 antennas x 2048 rays x 128 target samples (64 coarse), S = 256, "
+                        "MF at the target points, target |MF| of the shell + torus scene (49152 channels, 128^3)"),
+           "power": power, "mixed_graph": fast, "plain_eager": ref,
+           "speedup_at_equal_steps": fast["it_per_s"] / ref["it_per_s"],
+           "plain_final_chamfer_m": target,
+           "mixed_steps_to_plain_final_chamfer": reach}
+    if reach is not None:
+        t_fast = reach * fast["ms_per_step"] * 1e-3
+        t_ref = steps * ref["ms_per_step"] * 1e-3
+        out["mixed_seconds_to_plain_final_chamfer"] = t_fast
+        out["plain_seconds"] = t_ref
+        out["speedup_at_equal_chamfer"] = t_ref / t_fast
+    return out
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--checkpoints", type=int, default=8)
+    args = ap.parse_args(argv)
+    print(json.dumps(compare(args.steps, args.seed, args.checkpoints), indent=1))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

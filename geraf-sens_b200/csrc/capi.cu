@@ -37,7 +37,8 @@ int32_t cuda_fail(cudaError_t err, const char* what) {
 constexpr int kMaxDevices = 64;
 std::once_flag g_dev_once[kMaxDevices];
 DeviceInfo g_dev_info[kMaxDevices];
-int* g_status_ptr[kMaxDevices];
+std::mutex g_status_mutex;
+int* g_status_ptr[kMaxDevices];  // guarded by g_status_mutex; null until a lookup succeeds
 
 int current_device() {
   int dev = 0;
@@ -53,13 +54,6 @@ void init_device(int dev) {
   if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && v > 0)
     info.max_smem_optin = v;
   g_dev_info[dev] = info;
-  void* ptr = nullptr;
-  if (cudaGetSymbolAddress(&ptr, g_device_status) == cudaSuccess) {
-    g_status_ptr[dev] = static_cast<int*>(ptr);
-  } else {
-    g_status_ptr[dev] = nullptr;
-    cudaGetLastError();
-  }
 }
 
 void ensure_device(int dev) {
@@ -183,8 +177,22 @@ DeviceInfo current_device_info() {
 
 int* device_status_ptr() {
   const int dev = current_device();
-  ensure_device(dev);
+  // A successful lookup is kept per device; a failed one (e.g. made before the
+  // device could be used) is not, so the next call tries again.
+  std::lock_guard<std::mutex> lock(g_status_mutex);
+  if (g_status_ptr[dev] == nullptr) {
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_device_status) == cudaSuccess) {
+      g_status_ptr[dev] = static_cast<int*>(ptr);
+    } else {
+      cudaGetLastError();
+    }
+  }
   return g_status_ptr[dev];
+}
+
+int32_t mf_check_sizes(int64_t A, int64_t S, int64_t N, int32_t dtype, int32_t mode) {
+  return check_mf_sizes(A, S, N, dtype, mode);
 }
 
 PhaseConsts phase_consts(float f0, float As, float fs) {
@@ -677,4 +685,36 @@ GERAF_EXPORT int32_t geraf_bilinear_backward(const void* grad_output_normals,
   if (num_target_samples == 0) return GERAF_OK;
   return finish_launch(bilinear_backward(a, static_cast<cudaStream_t>(stream)),
                        "bilinear_raysample_backward launch");
+}
+
+// ---- matched-filter volume at target points --------------------------------
+GERAF_EXPORT int32_t geraf_volume_sample(const void* volume, int64_t nx, int64_t ny, int64_t nz,
+                                         const void* points_norm, int64_t num_points, void* out,
+                                         int32_t mode, int32_t align_corners, void* stream) {
+  REQUIRE(nx >= 0 && ny >= 0 && nz >= 0 && num_points >= 0, "sizes must be non-negative");
+  REQUIRE(nx <= kI32Max && ny <= kI32Max && nz <= kI32Max, "volume dimensions must fit int32");
+  REQUIRE(mode == GERAF_SAMPLE_TRILINEAR || mode == GERAF_SAMPLE_NEAREST,
+          "mode must be GERAF_SAMPLE_TRILINEAR or GERAF_SAMPLE_NEAREST");
+  const bool empty = nx == 0 || ny == 0 || nz == 0;
+  if (num_points > 0) {
+    REQUIRE(points_norm != nullptr && out != nullptr && (empty || volume != nullptr),
+            "pointers must be non-null");
+  }
+  if (num_points == 0) return GERAF_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (empty) {  // an empty volume samples to zero everywhere
+    return finish_launch(cudaMemsetAsync(out, 0, static_cast<size_t>(num_points) * sizeof(float), st),
+                         "volume_sample fill");
+  }
+  VolumeSampleArgs a{};
+  a.volume = volume;
+  a.points = points_norm;
+  a.out = out;
+  a.nx = nx;
+  a.ny = ny;
+  a.nz = nz;
+  a.num_points = num_points;
+  a.nearest = mode == GERAF_SAMPLE_NEAREST;
+  a.align_corners = align_corners != 0;
+  return finish_launch(volume_sample(a, st), "volume_sample launch");
 }

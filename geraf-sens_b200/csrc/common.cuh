@@ -118,14 +118,18 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
   return t;
 }
 
-// Waits for phase `parity` of `bar` for at most ~2 s of wall time.  Returns
-// false (and raises *status) when it gives up.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* status) {
+// Wall-time limit of every bounded wait of the operators (2 s).
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+
+// Waits for phase `parity` of `bar` for at most `limit_ns` of wall time (and at
+// most 2^26 polls).  Returns false (and raises *status) when it gives up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* status,
+                                                  uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = global_timer_ns();
   for (uint32_t it = 0; it < (1u << 26); ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 255u && global_timer_ns() - t0 > 2000000000ull) break;
+    if ((it & 255u) == 255u && global_timer_ns() - t0 > limit_ns) break;
   }
   if (status != nullptr) atomicExch(status, kStatusTimeout);
   return false;
@@ -144,6 +148,7 @@ struct PairStager {
   int ld;          // shared row stride in elements (multiple of 4)
   int rows_max;
   bool bulk;
+  uint64_t wait_ns = kWaitLimitNs;  // limit of each bounded wait
 
   __device__ __forceinline__ T* stage_ptr(int stage, int which) const {
     return buf + (static_cast<int64_t>(stage) * 2 + which) * rows_max * ld;
@@ -181,14 +186,14 @@ struct PairStager {
   // across the block, so the caller can return without stranding a barrier).
   __device__ __forceinline__ bool wait(int stage, uint32_t parity, int* status) {
     bool ok = true;
-    if (bulk) ok = mbar_wait_bounded(&bar[stage], parity, status);
+    if (bulk) ok = mbar_wait_bounded(&bar[stage], parity, status, wait_ns);
     return __syncthreads_and(ok) != 0;
   }
 
   // After a timeout: thread 0 waits (bounded) for a copy still in flight
   // into `stage`, so the block never exits with TMA writes pending.
   __device__ __forceinline__ void drain(int stage, uint32_t parity, int* status) {
-    if (bulk && threadIdx.x == 0) mbar_wait_bounded(&bar[stage], parity, status);
+    if (bulk && threadIdx.x == 0) mbar_wait_bounded(&bar[stage], parity, status, wait_ns);
   }
 };
 
@@ -252,8 +257,62 @@ __device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
   return d;
 }
 
+// Packed FP32 add and subtract on two lanes (add/sub.rn.f32x2, sm_100+).
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
+  float2 d;
+  asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+
+// acc[m] += s0 * z^m for m = 0 .. K-1, |z| = 1.
+//
+// Each real component of u_m = s0 z^m is A cos(m theta + c), so it obeys the
+// three-term (Chebyshev / Goertzel) recurrence u_{m+1} = 2 cos(theta) u_m - u_{m-1}:
+// one FMA per component per sample instead of the 4-operation complex product
+// of a rotator.  The (re, im) pair of one term runs in one packed register:
+// one fma.rn.f32x2 for the recurrence and one add/sub.rn.f32x2 for the
+// accumulation, 2 issue slots per (term, sample).  So that no negation is
+// issued, the recurrence carries x_m = sigma_m u_m with the sign pattern
+// sigma = (+, +, -, -, +, +, ...):  x_{m+1} = (+-2 cos theta) x_m + x_{m-1}
+// (coefficient +2cos for odd m+1, -2cos for even), and x_m is added for
+// m mod 4 in {0, 1}, subtracted for {2, 3}.  RN rounding is sign-symmetric,
+// so the sums are bit-identical to the scalar recurrence.  Rounding errors of
+// the recurrence grow at most ~m^2 eps (theta near 0 or pi) and ~m eps /
+// |sin theta| otherwise, which is why callers re-seed from exact phasors
+// every K samples.
+template <int K>
+__device__ __forceinline__ void rotate_accumulate(float2 s0, float2 z, float2 (&acc)[K]) {
+  static_assert(K >= 2, "the recurrence needs two seeds");
+  const float2 c2 = make_float2(2.0f * z.x, 2.0f * z.x);
+  const float2 nc2 = make_float2(-2.0f * z.x, -2.0f * z.x);
+  float2 xm1 = s0;
+  float2 x = cmul(s0, z);
+  acc[0] = fadd2(acc[0], xm1);
+  acc[1] = fadd2(acc[1], x);
+#pragma unroll
+  for (int m = 2; m < K; ++m) {
+    const float2 xn = ffma2((m & 1) ? c2 : nc2, x, xm1);
+    xm1 = x;
+    x = xn;
+    acc[m] = (m & 2) ? fsub2(acc[m], x) : fadd2(acc[m], x);
+  }
 }
 
 // Stages the tx and rx positions of `rws` antennas from a0 into slot `stage`

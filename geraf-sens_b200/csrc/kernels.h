@@ -29,11 +29,15 @@ struct DeviceInfo {
 DeviceInfo current_device_info();
 
 // Device address of the library's status word on the current device
-// (looked up once per device; null if the lookup failed).
+// (a successful lookup is cached per device; null while lookups fail).
 int* device_status_ptr();
 
 // Sets the calling thread's message returned by geraf_rf_last_error().
 void set_last_error(const char* msg);
+
+// The matched filter's size / dtype / mode validation of geraf_mf_forward
+// (GERAF_OK or an error code, with the message set).
+int32_t mf_check_sizes(int64_t A, int64_t S, int64_t N, int32_t dtype, int32_t mode);
 
 // ---- matched filter ------------------------------------------------------
 struct MfArgs {
@@ -171,6 +175,16 @@ struct BilinearArgs {
 };
 cudaError_t bilinear_forward(const BilinearArgs& a, cudaStream_t st);
 cudaError_t bilinear_backward(const BilinearArgs& a, cudaStream_t st);
+
+// ---- volume sampling at target points -----------------------------------------
+struct VolumeSampleArgs {
+  const void* volume;  // [nx, ny, nz] float32, x slowest
+  const void* points;  // [num_points, 3] float32, normalised (x, y, z)
+  void* out;           // [num_points] float32
+  int64_t nx, ny, nz, num_points;
+  bool nearest, align_corners;
+};
+cudaError_t volume_sample(const VolumeSampleArgs& a, cudaStream_t st);
 
 // ---- shared host helpers -------------------------------------------------
 // FP64 phase constants of the MIXED form for start frequency f0, chirp slope

@@ -15,7 +15,8 @@
 // MIXED kernels use that phi is linear in n: with z = exp(-j 2 pi dcyc) the
 // forward inner sum is exp(-j phi0) * P_a(z), P_a(z) = sum_n s[a,n] z^n,
 // evaluated by Horner (4 FMA per sample); the adjoint generates
-// G[v] exp(j phi0) zeta^n by a rotator recurrence.  phi0 is reduced modulo one
+// G[v] exp(j phi0) zeta^n by a three-term recurrence per real component,
+// re-seeded from exact phasors every K samples.  phi0 is reduced modulo one
 // cycle in FP64 (path_cycles), so only two phasors per (v, a) are evaluated.
 #include <algorithm>
 
@@ -378,9 +379,11 @@ struct MfBwdP {
 
 // MIXED adjoint.  Block = (antenna, voxel split, sample range).  Phase 1:
 // thread t forms w = G[v] exp(j phi0) and the group seeds w zeta^(g K) of
-// voxel v0 + t.  Phase 2: thread (group g, lane l) rotates seeds of its
-// lane's voxels through K samples, accumulating in registers; a two-level
-// FP32 sum (flushed per tile) bounds the error growth over long voxel ranges.
+// voxel v0 + t.  Phase 2: thread (group g, lane l) runs each seed of its
+// lane's voxels through K samples by the packed three-term recurrence
+// (rotate_accumulate: 2 issue slots per voxel-sample), accumulating in
+// registers; a two-level FP32 sum (flushed per tile) bounds the error growth
+// over long voxel ranges.
 template <typename T, int K>
 __global__ void __launch_bounds__(256) mf_bwd_mixed_kernel(const MfBwdP<T> p) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -401,9 +404,9 @@ __global__ void __launch_bounds__(256) mf_bwd_mixed_kernel(const MfBwdP<T> p) {
 
   const int g = threadIdx.x / L;
   const int l = threadIdx.x - g * L;
-  float accr[K], acci[K], hir[K], hii[K];
+  float2 acc[K], hi[K];
 #pragma unroll
-  for (int m = 0; m < K; ++m) accr[m] = acci[m] = hir[m] = hii[m] = 0.0f;
+  for (int m = 0; m < K; ++m) acc[m] = hi[m] = make_float2(0.0f, 0.0f);
 
   for (int64_t v0 = v_begin; v0 < v_end; v0 += TILE) {
     {  // phase 1
@@ -434,21 +437,11 @@ __global__ void __launch_bounds__(256) mf_bwd_mixed_kernel(const MfBwdP<T> p) {
     __syncthreads();
     {  // phase 2
       const int count = static_cast<int>(min(static_cast<int64_t>(TILE), v_end - v0));
-      for (int vl = l; vl < count; vl += L) {
-        float2 s = seeds[g * TILE + vl];
-        const float2 z = zeta[vl];
-#pragma unroll
-        for (int m = 0; m < K; ++m) {
-          accr[m] += s.x;
-          acci[m] += s.y;
-          s = cmul(s, z);
-        }
-      }
+      for (int vl = l; vl < count; vl += L) rotate_accumulate<K>(seeds[g * TILE + vl], zeta[vl], acc);
 #pragma unroll
       for (int m = 0; m < K; ++m) {
-        hir[m] += accr[m];
-        hii[m] += acci[m];
-        accr[m] = acci[m] = 0.0f;
+        hi[m] = fadd2(hi[m], acc[m]);
+        acc[m] = make_float2(0.0f, 0.0f);
       }
     }
     __syncthreads();
@@ -457,7 +450,7 @@ __global__ void __launch_bounds__(256) mf_bwd_mixed_kernel(const MfBwdP<T> p) {
   // Reduce the L lanes of each group through shared memory (fixed order).
   float2* red = reinterpret_cast<float2*>(smem);  // [G][K][L]
 #pragma unroll
-  for (int m = 0; m < K; ++m) red[(g * K + m) * L + l] = make_float2(hir[m], hii[m]);
+  for (int m = 0; m < K; ++m) red[(g * K + m) * L + l] = hi[m];
   __syncthreads();
   for (int idx = threadIdx.x; idx < G * K; idx += blockDim.x) {
     const int64_t n = n_begin + idx;

@@ -32,18 +32,26 @@ constexpr int kMinSplits = 2;
 static __device__ __align__(256) float2 g_noalloc_scratch[kMaxSlots];
 
 constexpr int kMaxDevices = 64;
-std::once_flag g_once[kMaxDevices];
-void* g_scratch_ptr[kMaxDevices];
-cudaError_t g_scratch_err[kMaxDevices];
+std::mutex g_scratch_mutex;
+void* g_scratch_ptr[kMaxDevices];  // guarded by g_scratch_mutex; null until a lookup succeeds
 
 // In host code `g_noalloc_scratch` names a host-side shadow, not device
-// memory: the device address must be looked up, once per device, with that
-// device current.
-void init_scratch(int dev) {
-  void* p = nullptr;
-  g_scratch_err[dev] = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-  g_scratch_ptr[dev] = g_scratch_err[dev] == cudaSuccess ? p : nullptr;
-  if (g_scratch_err[dev] != cudaSuccess) cudaGetLastError();
+// memory: the device address is looked up with the device current.  A
+// successful lookup is kept per device; a failed one (e.g. made before the
+// device could be used) is not, so the next call tries again.
+void* scratch_address(int dev, cudaError_t* err) {
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  *err = cudaSuccess;
+  if (g_scratch_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    *err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (*err != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    g_scratch_ptr[dev] = p;
+  }
+  return g_scratch_ptr[dev];
 }
 
 int32_t fail(int32_t code, const std::string& msg) {
@@ -63,12 +71,11 @@ GERAF_EXPORT int32_t geraf_mf_forward_noalloc(const void* real, const void* imag
                                               int64_t num_adc_samples, float adc_sample_rate,
                                               float chirp_slope_scaled, int64_t num_voxels,
                                               void* stream) {
-  if (total_ant_size < 0 || num_adc_samples < 0 || num_voxels < 0 ||
-      total_ant_size > 2147483647LL || num_adc_samples > 2147483647LL) {
-    return fail(GERAF_ERR_INVALID_ARGUMENT,
-                "sizes must be non-negative and fit the reference's int arguments");
+  if (int32_t rc = mf_check_sizes(total_ant_size, num_adc_samples, num_voxels, GERAF_DTYPE_F32,
+                                  GERAF_MODE_MIXED)) {
+    return rc;
   }
-  if (num_voxels * kMinSplits > kMaxSlots) {
+  if (num_voxels > kMaxSlots / kMinSplits) {
     return fail(GERAF_ERR_INVALID_ARGUMENT,
                 "num_voxels " + std::to_string(num_voxels) +
                     " exceeds the fixed scratch of geraf_mf_forward_noalloc (at most " +
@@ -86,10 +93,9 @@ GERAF_EXPORT int32_t geraf_mf_forward_noalloc(const void* real, const void* imag
   if (err != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     return fail(GERAF_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(err));
   }
-  std::call_once(g_once[dev], init_scratch, dev);
-  if (g_scratch_ptr[dev] == nullptr) {
-    return fail(GERAF_ERR_CUDA,
-                std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(g_scratch_err[dev]));
+  void* scratch = scratch_address(dev, &err);
+  if (scratch == nullptr) {
+    return fail(GERAF_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(err));
   }
 
   MfArgs a{};
@@ -115,7 +121,7 @@ GERAF_EXPORT int32_t geraf_mf_forward_noalloc(const void* real, const void* imag
   if (t.splits < kMinSplits) t.splits = kMinSplits;
   // Every (split, voxel) slot is written before the finishing pass reads it,
   // so the scratch needs no clearing between calls.
-  err = mf_forward(a, t, g_scratch_ptr[dev], static_cast<cudaStream_t>(stream));
+  err = mf_forward(a, t, scratch, static_cast<cudaStream_t>(stream));
   if (err != cudaSuccess) {
     return fail(GERAF_ERR_CUDA,
                 std::string("matched_filter_forward_noalloc launch: ") + cudaGetErrorString(err));

@@ -162,9 +162,9 @@ __global__ void __launch_bounds__(256) ragged_fwd_kernel(const RgP<T> p) {
     ld3(p.rx, a, rxp);
     const double tx = txp[0], ty = txp[1], tz = txp[2], rx = rxp[0], ry = rxp[1], rz = rxp[2];
 
-    float accr[K], acci[K], hir[K], hii[K];
+    float2 acc[K], hi[K];
 #pragma unroll
-    for (int m = 0; m < K; ++m) accr[m] = acci[m] = hir[m] = hii[m] = 0.0f;
+    for (int m = 0; m < K; ++m) acc[m] = hi[m] = make_float2(0.0f, 0.0f);
 
     // The point data of tile k + 1 are loaded while tile k's samples are summed.
     float nrm[3] = {0.0f, 0.0f, 1.0f}, pt[3] = {0.0f, 0.0f, 0.0f}, sig = 0.0f;
@@ -222,28 +222,18 @@ __global__ void __launch_bounds__(256) ragged_fwd_kernel(const RgP<T> p) {
       }
       load_point(p0 + TILE + threadIdx.x);  // in flight during the sums below
       __syncthreads();
-      for (int vl = l; vl < count; vl += L) {
-        float2 s = seeds[g * TILE + vl];
-        const float2 z = zeta[vl];
-#pragma unroll
-        for (int m = 0; m < K; ++m) {
-          accr[m] += s.x;
-          acci[m] += s.y;
-          s = cmul(s, z);
-        }
-      }
+      for (int vl = l; vl < count; vl += L) rotate_accumulate<K>(seeds[g * TILE + vl], zeta[vl], acc);
 #pragma unroll
       for (int m = 0; m < K; ++m) {
-        hir[m] += accr[m];
-        hii[m] += acci[m];
-        accr[m] = acci[m] = 0.0f;
+        hi[m] = fadd2(hi[m], acc[m]);
+        acc[m] = make_float2(0.0f, 0.0f);
       }
       __syncthreads();
     }
     // Reduce the lanes of each sample group and store this item's partial row.
     float2* red = reinterpret_cast<float2*>(smem);  // [G][K][L]
 #pragma unroll
-    for (int m = 0; m < K; ++m) red[(g * K + m) * L + l] = make_float2(hir[m], hii[m]);
+    for (int m = 0; m < K; ++m) red[(g * K + m) * L + l] = hi[m];
     __syncthreads();
     for (int idx = threadIdx.x; idx < G * K; idx += blockDim.x) {
       if (idx >= p.S) continue;

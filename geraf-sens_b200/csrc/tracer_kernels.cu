@@ -14,8 +14,8 @@
 // are bit-identical -- and the sample loop works on (amplitude, delay) only.
 // PLAIN forms then evaluate the reference's per-sample phase with accurate
 // cosf/sinf in its summation order; MIXED forms reduce the carrier phase in
-// FP64 and generate the per-sample phasors with a rotator (forward) or a
-// Horner recurrence (adjoint), which also yields the position gradient the
+// FP64 and generate the per-sample phasors with a three-term recurrence
+// (forward) or a Horner recurrence (adjoint), which also yields the position gradient the
 // reference does not provide.
 #include <algorithm>
 
@@ -131,7 +131,8 @@ __global__ void __launch_bounds__(128) tracer_fwd_plain_kernel(const TrP<T> p) {
 // thread t forms the geometry of point p0 + t, culled and out-of-bounds
 // points are compacted away, and each surviving point stores its group seeds
 // amp exp(j phi(n_g)) and its per-sample rotator zeta.  Phase 2: thread
-// (group g, lane l) rotates the seeds of its lane's points through K samples.
+// (group g, lane l) runs the seeds of its lane's points through K samples
+// (rotate_accumulate: packed three-term recurrence).
 template <typename T, int K>
 __global__ void __launch_bounds__(256) tracer_fwd_mixed_kernel(const TrP<T> p) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -158,9 +159,9 @@ __global__ void __launch_bounds__(256) tracer_fwd_mixed_kernel(const TrP<T> p) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
-  float accr[K], acci[K], hir[K], hii[K];
+  float2 acc[K], hi[K];
 #pragma unroll
-  for (int m = 0; m < K; ++m) accr[m] = acci[m] = hir[m] = hii[m] = 0.0f;
+  for (int m = 0; m < K; ++m) acc[m] = hi[m] = make_float2(0.0f, 0.0f);
 
   // The point data of tile k + 1 are loaded while tile k's samples are summed.
   float nrm[3] = {0.0f, 0.0f, 1.0f}, pt[3] = {0.0f, 0.0f, 0.0f}, sig = 0.0f;
@@ -224,28 +225,18 @@ __global__ void __launch_bounds__(256) tracer_fwd_mixed_kernel(const TrP<T> p) {
     }
     load_point(p0 + TILE + threadIdx.x);  // in flight during the sums below
     __syncthreads();
-    for (int vl = l; vl < count; vl += L) {
-      float2 s = seeds[g * TILE + vl];
-      const float2 z = zeta[vl];
-#pragma unroll
-      for (int m = 0; m < K; ++m) {
-        accr[m] += s.x;
-        acci[m] += s.y;
-        s = cmul(s, z);
-      }
-    }
+    for (int vl = l; vl < count; vl += L) rotate_accumulate<K>(seeds[g * TILE + vl], zeta[vl], acc);
 #pragma unroll
     for (int m = 0; m < K; ++m) {
-      hir[m] += accr[m];
-      hii[m] += acci[m];
-      accr[m] = acci[m] = 0.0f;
+      hi[m] = fadd2(hi[m], acc[m]);
+      acc[m] = make_float2(0.0f, 0.0f);
     }
     __syncthreads();
   }
 
   float2* red = reinterpret_cast<float2*>(smem);  // [G][K][L]
 #pragma unroll
-  for (int m = 0; m < K; ++m) red[(g * K + m) * L + l] = make_float2(hir[m], hii[m]);
+  for (int m = 0; m < K; ++m) red[(g * K + m) * L + l] = hi[m];
   __syncthreads();
   for (int idx = threadIdx.x; idx < G * K; idx += blockDim.x) {
     const int64_t n = n_begin + idx;

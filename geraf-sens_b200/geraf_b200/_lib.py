@@ -29,6 +29,9 @@ MODE_PLAIN = 0
 MODE_MIXED = 1
 MODE_NUFFT = 2
 
+SAMPLE_TRILINEAR = 0
+SAMPLE_NEAREST = 1
+
 
 class Tuning(ctypes.Structure):
     """``geraf_tuning_t``: launch shape; 0 in any field = library default."""
@@ -67,9 +70,6 @@ SIGNATURES = {
     "geraf_rf_cudart_version": (_i32, []),
     "geraf_rf_build_info": (ctypes.c_char_p, []),
     "geraf_rf_device_status": (_i32, [_vp, _i32, ctypes.POINTER(_i32)]),
-    "geraf_rf_fma_probe": (_i32, [_i32, _i32, _i32, _vp, _vp]),
-    "geraf_rf_horner_probe": (_i32, [_i32, _i32, _i32, _vp, _vp]),
-    "geraf_rf_sincos_identity_check": (_i32, [_vp, _vp]),
     "geraf_mf_forward_workspace_bytes": (_i32, [_i64, _i64, _i64, _i32, _i32, _tp, _szp]),
     "geraf_mf_forward": (
         _i32,
@@ -124,6 +124,12 @@ SIGNATURES = {
     "geraf_bilinear_backward": (
         _i32, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i32, _vp]
     ),
+    "geraf_volume_sample": (_i32, [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _i32, _i32, _vp]),
+}
+
+# Test hooks (include/geraf_rf_testing.h): not operators, bound for the tests.
+TEST_SIGNATURES = {
+    "geraf_rf_selftest_wait_timeout": (_i32, [_i64, _i32, _vp, _vp]),
 }
 
 _lock = threading.Lock()
@@ -152,7 +158,7 @@ def load() -> ctypes.CDLL:
                 "`make -C geraf-sens_b200/csrc` (or __graft_entry__.build())"
             )
         lib = ctypes.CDLL(LIB_PATH)
-        for name, (restype, argtypes) in SIGNATURES.items():
+        for name, (restype, argtypes) in {**SIGNATURES, **TEST_SIGNATURES}.items():
             fn = getattr(lib, name)
             fn.restype = restype
             fn.argtypes = argtypes

@@ -114,7 +114,7 @@ def mf_forward_candidates(mode: int) -> list[dict]:
 
 def sample_major_candidates() -> list[dict]:
     """MF adjoint / tracer forward: threads x samples-per-lane."""
-    return [{"threads": t, "chunk": c} for t in (128, 256) for c in (8, 16, 32)]
+    return [{"threads": t, "chunk": c} for t in (64, 128, 256) for c in (8, 16, 32)]
 
 
 def tracer_backward_candidates() -> list[dict]:

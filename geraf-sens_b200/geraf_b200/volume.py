@@ -120,15 +120,32 @@ def process_object(obj_dir: str, adc_sample_rate: float, As_sci: float, bound, m
 
 def sample_volume(volume: torch.Tensor, points_norm: torch.Tensor, mode: str = "bilinear",
                   align_corners: bool = True) -> torch.Tensor:
-    """Samples an (Nx, Ny, Nz) volume at points in normalised [-1, 1]^3 (x, y, z) coordinates
-    on the volume's device -- the reference's ``_sample_volume``
-    (``geraf/datasets/transforms/loading.py:20-25``), which runs on the host in the
-    data workers, moved next to the matched-filter output."""
-    vol = volume.to(torch.float32)
-    pts = points_norm.to(device=vol.device, dtype=torch.float32).reshape(-1, 3)
-    grid = torch.stack([pts[:, 2], pts[:, 1], pts[:, 0]], -1).view(1, 1, 1, -1, 3)
-    out = torch.nn.functional.grid_sample(vol[None, None], grid, mode=mode, align_corners=align_corners)
-    return out.reshape(-1)
+    """Samples an (Nx, Ny, Nz) volume at points in normalised [-1, 1]^3 (x, y, z)
+    coordinates on the GPU -- the reference's ``_sample_volume`` /
+    ``InterpolateMFAtTargets`` (``geraf/datasets/transforms/loading.py:20-25,
+    78-100``), which run torch grid_sample on the host in the data workers,
+    moved next to the matched-filter output.  ``mode`` "bilinear" (trilinear)
+    or "nearest", zeros outside the volume.  Both tensors must be CUDA tensors
+    on one device; returns float32 [P] there (the library kernel
+    ``geraf_volume_sample``: no PyTorch fallback)."""
+    from . import _lib
+    from .runtime import device_guard, ptr, stream_ptr
+
+    modes = {"bilinear": _lib.SAMPLE_TRILINEAR, "nearest": _lib.SAMPLE_NEAREST}
+    if mode not in modes:
+        raise ValueError(f"sample_volume supports modes {sorted(modes)}, not {mode!r}")
+    if volume.dim() != 3:
+        raise ValueError(f"`volume` must have shape [Nx, Ny, Nz], got {tuple(volume.shape)}")
+    if not (volume.is_cuda and points_norm.is_cuda) or volume.device != points_norm.device:
+        raise ValueError("`volume` and `points_norm` must be CUDA tensors on the same device")
+    vol = volume.to(torch.float32).contiguous()
+    pts = points_norm.to(torch.float32).reshape(-1, 3).contiguous()
+    out = torch.empty(pts.shape[0], dtype=torch.float32, device=vol.device)
+    nx, ny, nz = vol.shape
+    with device_guard(vol.device):
+        _lib.call("geraf_volume_sample", ptr(vol), nx, ny, nz, ptr(pts), pts.shape[0], ptr(out), modes[mode],
+                  int(bool(align_corners)), stream_ptr(vol.device))
+    return out
 
 
 def main(argv=None) -> int:

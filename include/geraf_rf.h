@@ -88,29 +88,6 @@ int32_t geraf_rf_cudart_version(void);
 /* Compiler and target description, e.g. "GCC 13.3; nvcc 12.9; sm_100a"
  * (reference: csrc/vision.cpp:47-68, get_compiler_version). */
 const char* geraf_rf_build_info(void);
-/* Measures nothing itself: enqueues blocks x threads threads (threads <= 256)
- * of `iters` iterations of 8 independent packed FP32 FMAs (2 FMAs each), i.e.
- * blocks*threads*iters*32 flops, for timing by the caller.  `sink` is device memory of blocks*threads
- * floats (never written in practice).  The FP32-pipe roofline denominator of
- * the RF kernels; no counterpart in the reference. */
-int32_t geraf_rf_fma_probe(int32_t blocks, int32_t threads, int32_t iters, float* sink,
-                           void* stream);
-/* Enqueues blocks x threads threads (threads <= 128) of the MIXED matched
- * filter forward's Horner loop alone -- 8 voxels per thread in packed pairs,
- * `rows` rows of 256 shared-memory samples, no per-(voxel, antenna) phase
- * set-up -- i.e. blocks*threads*rows*16384 flops, for timing by the caller.
- * The ceiling of that loop's instruction form, reported beside the FMA-rate
- * roofline; `sink` as above.  No counterpart in the reference. */
-int32_t geraf_rf_horner_probe(int32_t blocks, int32_t threads, int32_t rows, float* sink,
-                              void* stream);
-/* Enqueues a check of every FP32 input (all 2^32 bit patterns): adds to
- * *mismatches (device memory, zeroed by the caller) the number of inputs for
- * which sincosf differs in any bit from separate sinf and cosf calls.  The
- * PLAIN kernels take cos and sin of each phase from one sincosf call where the
- * reference calls cosf and sinf (MatchedFilter_cuda_kernel.cu:60-63,
- * SignalTracer_cuda_kernel.cu:442-443, 555-556); their bit-exactness rests on
- * this count being zero.  No counterpart in the reference. */
-int32_t geraf_rf_sincos_identity_check(unsigned long long* mismatches, void* stream);
 /* Reads, and with reset != 0 clears, the device status word of the current
  * device: GERAF_OK, or the code a kernel raised -- GERAF_ERR_DEVICE_TIMEOUT
  * (a bounded wait gave up), GERAF_ERR_INVALID_ARGUMENT (malformed ragged
@@ -292,6 +269,22 @@ int32_t geraf_bilinear_backward(const void* grad_output_normals, const void* gra
                                 void* grad_normals, void* grad_sigmas, int64_t num_antennas,
                                 int64_t num_rays, int64_t num_samples,
                                 int64_t num_target_samples, int32_t dtype, void* stream);
+
+/* ---- matched-filter volume at target points ----------------------------- */
+/* out[i] = the volume [nx, ny, nz] (float32, x slowest, as sarimage.bin) sampled
+ * at points_norm[i] = (x, y, z) in normalised [-1, 1]^3 coordinates: trilinear
+ * (mode GERAF_SAMPLE_TRILINEAR) or nearest-voxel (GERAF_SAMPLE_NEAREST, ties to
+ * even), zero outside the volume, corners at +-1 when align_corners != 0.
+ * points_norm [num_points, 3] and out [num_points] are float32.  The torch
+ * grid_sample call of the reference's data workers: the volume as a
+ * [1,1,nx,ny,nz] tensor with the grid given as (z, y, x), padding zeros.
+ * Replaces _sample_volume / InterpolateMFAtTargets
+ * (geraf/datasets/transforms/loading.py:20-25, 78-100), which run on the host. */
+#define GERAF_SAMPLE_TRILINEAR 0
+#define GERAF_SAMPLE_NEAREST 1
+int32_t geraf_volume_sample(const void* volume, int64_t nx, int64_t ny, int64_t nz,
+                            const void* points_norm, int64_t num_points, void* out, int32_t mode,
+                            int32_t align_corners, void* stream);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -45,6 +45,8 @@ def lib():
         L.oracle_mf_forward_f32.argtypes = mf + [_f32p, _f32p]
         L.oracle_mf_backward_f64.argtypes = mf + [_f64p, _f64p]
         L.oracle_mf_backward_f32.argtypes = mf + [_f32p, _f32p]
+        L.oracle_mf_forward_f64r.argtypes = mf + [_f64p, _f64p]
+        L.oracle_mf_backward_f64r.argtypes = mf + [_f64p, _f64p]
         fft = [_f32p, _f32p, _f32p, _f32p, _f32p, _i64, _i64, _i64, _f, _f32p, _f32p]
         L.oracle_mf_fft_forward_f32.argtypes = fft
         L.oracle_mf_fft_backward_f32.argtypes = fft
@@ -76,28 +78,37 @@ def _u8(x) -> np.ndarray:
 
 
 # ---- matched filter ---------------------------------------------------------
+def _mf_fn(kind, form):
+    if form not in ("f64", "f64r", "f32"):
+        raise ValueError(f"unknown oracle form {form!r}")
+    return getattr(lib(), f"oracle_mf_{kind}_{form}")
+
+
 def mf_forward(real, imag, tx, rx, voxel_3n, fs, As, form="f64"):
-    """y[N] complex of the matched filter (MatchedFilter_cuda_kernel.cu:65-115)."""
+    """y[N] complex of the matched filter (MatchedFilter_cuda_kernel.cu:65-115).
+
+    ``form``: "f64" (libm cos/sin per sample), "f64r" (the same FP64 model with
+    phasors by FP64 rotation, re-seeded every 16 samples; for full-size
+    workloads) or "f32" (the reference's FP32 order)."""
     real, imag, tx, rx, vox = map(_f32, (real, imag, tx, rx, voxel_3n))
     A, S = real.shape
     N = vox.shape[1]
-    dt = np.float64 if form == "f64" else np.float32
+    dt = np.float32 if form == "f32" else np.float64
     out_r = np.zeros(N, dt)
     out_i = np.zeros(N, dt)
-    fn = lib().oracle_mf_forward_f64 if form == "f64" else lib().oracle_mf_forward_f32
-    fn(real, imag, tx, rx, vox, A, S, N, fs, As, out_r, out_i)
+    _mf_fn("forward", form)(real, imag, tx, rx, vox, A, S, N, fs, As, out_r, out_i)
     return out_r, out_i
 
 
 def mf_backward(grad_r, grad_i, tx, rx, voxel_3n, A, S, fs, As, form="f64"):
-    """grad[A,S] complex of the adjoint (MatchedFilter_cuda_kernel.cu:171-220)."""
+    """grad[A,S] complex of the adjoint (MatchedFilter_cuda_kernel.cu:171-220);
+    ``form`` as for :func:`mf_forward`."""
     gr, gi, tx, rx, vox = map(_f32, (grad_r, grad_i, tx, rx, voxel_3n))
     N = vox.shape[1]
-    dt = np.float64 if form == "f64" else np.float32
+    dt = np.float32 if form == "f32" else np.float64
     out_r = np.zeros((A, S), dt)
     out_i = np.zeros((A, S), dt)
-    fn = lib().oracle_mf_backward_f64 if form == "f64" else lib().oracle_mf_backward_f32
-    fn(gr, gi, tx, rx, vox, A, S, N, fs, As, out_r, out_i)
+    _mf_fn("backward", form)(gr, gi, tx, rx, vox, A, S, N, fs, As, out_r, out_i)
     return out_r, out_i
 
 
@@ -181,3 +192,45 @@ def bilinear_backward(grad_out_normals, grad_out_sigmas, z_vals, tgt_z_vals, gra
     gs = _f32(grad_sigmas).copy() if grad_sigmas is not None else np.zeros((A, R, S), np.float32)
     lib().oracle_bilinear_backward_f32(gon, gos, z, tz, A, R, S, T, gn, gs)
     return gn, gs
+
+
+# ---- matched-filter volume at target points ---------------------------------
+def sample_volume(volume, points_norm, mode="bilinear", align_corners=True):
+    """FP64 restatement of the reference's ``_sample_volume``
+    (geraf/datasets/transforms/loading.py:20-25): torch ``grid_sample`` (the
+    published 3-D algorithm of torch, pinned at 2.4.1 by the reference) of a
+    [1,1,Nx,Ny,Nz] volume at a grid given as (z, y, x) -- so normalised x
+    selects along Nx -- with zero padding; ``mode`` "bilinear" (trilinear in
+    3-D) or "nearest" (ties to even).  Returns float64 [P]."""
+    vol = np.asarray(volume, np.float64)
+    pts = np.asarray(points_norm, np.float64).reshape(-1, 3)
+    dims = vol.shape
+
+    def src(c, n):
+        return (c + 1.0) * 0.5 * (n - 1) if align_corners else ((c + 1.0) * n - 1.0) * 0.5
+
+    f = [src(pts[:, k], dims[k]) for k in range(3)]
+    out = np.zeros(pts.shape[0])
+
+    def gather(idx):
+        ok = np.ones(pts.shape[0], bool)
+        for k in range(3):
+            ok &= (idx[k] >= 0) & (idx[k] < dims[k])
+        vals = np.zeros(pts.shape[0])
+        safe = [np.where(ok, idx[k], 0).astype(np.int64) for k in range(3)]
+        vals[ok] = vol[safe[0][ok], safe[1][ok], safe[2][ok]]
+        return vals
+
+    if mode == "nearest":
+        return gather([np.rint(f[k]) for k in range(3)])  # numpy rint rounds half to even
+    if mode != "bilinear":
+        raise ValueError(f"unsupported mode {mode!r}")
+    lo = [np.floor(f[k]) for k in range(3)]
+    w1 = [f[k] - lo[k] for k in range(3)]
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                w = ((w1[0] if dx else 1 - w1[0]) * (w1[1] if dy else 1 - w1[1]) *
+                     (w1[2] if dz else 1 - w1[2]))
+                out += w * gather([lo[0] + dx, lo[1] + dy, lo[2] + dz])
+    return out

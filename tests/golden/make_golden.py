@@ -10,6 +10,7 @@ resampler's adjoint accumulates, so its gradient buffers start from a stored
 non-zero pattern.
 
     python tests/golden/make_golden.py --out tests/golden
+    python tests/golden/make_golden.py --only mf_3072ch_f32   # one case
 """
 from __future__ import annotations
 
@@ -23,7 +24,7 @@ import torch
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path[:0] = [ROOT, os.path.join(ROOT, "geraf-sens_b200")]
 
-from geraf_b200 import scenes  # noqa: E402
+from benchkit import scenes  # noqa: E402
 from oracle import build_ref  # noqa: E402
 
 
@@ -159,17 +160,57 @@ def run_bilinear(mod, inp):
                 grad_sigmas=gs.cpu().numpy())
 
 
+def run_mf_3072ch(mod):
+    """The reference's kernels on the full 3072-channel workload (3072 x 128 x 48^3).
+    The inputs are regenerated by the tests from their seed, so the fixture
+    keeps only checksums of them, the forward at the 4096-voxel subset and the
+    adjoint (of a seeded output gradient) at the 96-row subset."""
+    from oracle import workload_parity as wp
+
+    w = wp.mf3072_inputs(0)
+    A, S = w["re"].shape
+    N = w["vox"].shape[1]
+    args = [cu(w[k]) for k in ("re", "im", "tx", "rx")]
+    vox = cu(w["vox"])
+    out_r = torch.full((N,), float("nan"), device="cuda")
+    out_i = torch.full((N,), float("nan"), device="cuda")
+    mod.MatchedFilter_forward(*args, out_r, out_i, vox, A, S, float(w["fs"]), float(w["As"]), N)
+    g = wp.adjoint_grad(N, 21)
+    g_r = torch.full((A, S), float("nan"), device="cuda")
+    g_i = torch.full((A, S), float("nan"), device="cuda")
+    mod.MatchedFilter_backward_realimag(cu(g.real.copy()), cu(g.imag.copy()), *args, g_r, g_i, vox, A, S,
+                                        float(w["fs"]), float(w["As"]), N)
+    torch.cuda.synchronize()
+    vi, rows = wp.MF3072_VOXELS, wp.MF3072_ROWS
+    return dict(input_abs_sums=np.array([np.abs(w["re"].astype(np.float64)).sum(),
+                                         np.abs(w["im"].astype(np.float64)).sum()]),
+                voxel_ids=vi, rows=rows, grad_seed=np.int64(21),
+                out_real=out_r.cpu().numpy()[vi], out_imag=out_i.cpu().numpy()[vi],
+                grad_real=g_r.cpu().numpy()[rows], grad_imag=g_i.cpu().numpy()[rows])
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
+    ap.add_argument("--only", default=None, help="comma list of case names to (re)generate")
     args = ap.parse_args(argv)
     os.makedirs(args.out, exist_ok=True)
     mf = build_ref.load("RFMatchedFilter")
     st = build_ref.load("RFSignalTracer")
+    only = set(args.only.split(",")) if args.only else None
 
     def save(name, d):
         np.savez_compressed(os.path.join(args.out, name + ".npz"), **d)
         print("wrote", name)
+
+    if only is not None:
+        cases = {"mf_3072ch_f32": lambda: run_mf_3072ch(mf)}
+        unknown = only - set(cases)
+        if unknown:
+            raise SystemExit(f"--only supports {sorted(cases)}, not {sorted(unknown)}")
+        for name in sorted(only):
+            save(name, cases[name]())
+        return
 
     # matched filter: a physical scene, odd sizes, and the f16 / f64 dispatch paths
     inp = mf_inputs(1, scan=4, S=64, k=8, n=7)
@@ -193,6 +234,9 @@ def main(argv=None):
 
     inp = bilinear_inputs(8, A=2, R=12, S=16, T=24)
     save("bilinear_f32", {**inp, **run_bilinear(st, inp)})
+
+    # the reference's kernels at the full 3072-channel workload size
+    save("mf_3072ch_f32", run_mf_3072ch(mf))
 
 
 if __name__ == "__main__":

@@ -11,10 +11,11 @@ import pytest
 from conftest import ROOT
 
 HEADER = os.path.join(ROOT, "include", "geraf_rf.h")
+TESTING_HEADER = os.path.join(ROOT, "include", "geraf_rf_testing.h")
 
 
-def header_functions():
-    text = open(HEADER).read()
+def header_functions(path=HEADER):
+    text = open(path).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     decls = re.findall(r"\b(?:int32_t|const char\*)\s+(geraf_\w+)\s*\(([^;]*?)\)\s*;", text, flags=re.S)
     return {name: [a.strip() for a in args.split(",") if a.strip() and a.strip() != "void"]
@@ -24,24 +25,54 @@ def header_functions():
 def test_header_parses():
     fns = header_functions()
     assert "geraf_mf_forward" in fns and "geraf_tracer_backward" in fns
-    assert len(fns) == 23
+    assert len(fns) == 21
+    assert list(header_functions(TESTING_HEADER)) == ["geraf_rf_selftest_wait_timeout"]
 
 
 def test_library_exports_every_declared_symbol():
     from geraf_b200 import _lib
 
     lib = _lib.load()
-    for name in header_functions():
+    for name in list(header_functions()) + list(header_functions(TESTING_HEADER)):
         assert hasattr(lib, name), name
 
 
 def test_ctypes_signatures_match_header():
     from geraf_b200 import _lib
 
-    fns = header_functions()
-    assert set(fns) == set(_lib.SIGNATURES)
-    for name, args in fns.items():
-        assert len(_lib.SIGNATURES[name][1]) == len(args), name
+    for path, table in ((HEADER, _lib.SIGNATURES), (TESTING_HEADER, _lib.TEST_SIGNATURES)):
+        fns = header_functions(path)
+        assert set(fns) == set(table)
+        for name, args in fns.items():
+            assert len(table[name][1]) == len(args), name
+
+
+def test_measurement_probes_are_not_in_the_operator_library():
+    """The FP32 peak probes live in benchkit's libgeraf_probe.so, not here."""
+    from geraf_b200 import _lib
+
+    lib = _lib.load()
+    for name in ("geraf_rf_fma_probe", "geraf_rf_horner_probe", "geraf_rf_sincos_identity_check"):
+        assert not hasattr(lib, name), name
+
+
+def test_probe_library_exports_its_probes():
+    from benchkit import probes
+
+    lib = probes.lib()
+    for name in probes.SIGNATURES:
+        assert hasattr(lib, name), name
+
+
+def test_selftest_rejects_bad_arguments_without_gpu():
+    from geraf_b200 import _lib
+
+    lib = _lib.load()
+    fn = lib.geraf_rf_selftest_wait_timeout
+    assert fn(0, 1, 8, None) == _lib.GERAF_ERR_INVALID_ARGUMENT          # no limit
+    assert fn(3_000_000_000, 1, 8, None) == _lib.GERAF_ERR_INVALID_ARGUMENT  # above the operators' 2 s
+    assert fn(1_000_000, 0, 8, None) == _lib.GERAF_ERR_INVALID_ARGUMENT  # no blocks
+    assert fn(1_000_000, 1, None, None) == _lib.GERAF_ERR_INVALID_ARGUMENT
 
 
 def test_info_entry_points_run_without_gpu():

@@ -54,7 +54,7 @@ def oracle_tr_bwd(gr, gi, normals, sigmas, points, tx, rx, inb, S, fs, f0, As, p
 
 
 def make_inputs():
-    from geraf_b200 import scenes
+    from benchkit import scenes
 
     rng = np.random.default_rng(0)
     tx, rx = scenes.virtual_array(3)

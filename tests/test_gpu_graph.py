@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 import torch
 
-from geraf_b200 import scenes
+from benchkit import scenes
 
 pytestmark = pytest.mark.gpu
 
@@ -50,7 +50,7 @@ def test_ragged_step_graph_replay_equals_eager(cuda):
 
 @pytest.mark.parametrize("precision", ["mixed", "plain"])
 def test_stage1_step_graph_matches_eager_and_trains(cuda, precision):
-    from geraf_b200.step import Stage1RFStep
+    from benchkit.stage1 import Stage1RFStep
 
     kw = dict(num_antennas=8, num_rays=128, samples_per_ray=32, num_adc=32, precision=precision, seed=3)
     eager = Stage1RFStep(**kw)
@@ -69,7 +69,7 @@ def test_stage1_antenna_bank_matches_full_step_and_replays(cuda):
     """With the network unchanged, the banked step's first loss equals the full
     step's (the bank holds every chunk rendered by the same network); the banked
     step rotates through its chunks identically eager and graph-replayed."""
-    from geraf_b200.step import Stage1RFStep
+    from benchkit.stage1 import Stage1RFStep
 
     kw = dict(num_antennas=8, num_rays=128, samples_per_ray=32, num_adc=32, precision="mixed", seed=5)
     full = Stage1RFStep(**kw).run().item()

@@ -6,7 +6,7 @@ import pytest
 import torch
 
 from conftest import rel_l2
-from geraf_b200 import scenes
+from benchkit import scenes
 from gpu_helpers import cu, mf_backward, mf_forward
 from oracle import rf_oracle as orc
 

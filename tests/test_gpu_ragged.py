@@ -7,7 +7,8 @@ import pytest
 import torch
 
 from conftest import rel_l2
-from geraf_b200 import _lib, scenes
+from benchkit import scenes
+from geraf_b200 import _lib
 from oracle import rf_oracle as orc
 
 pytestmark = pytest.mark.gpu

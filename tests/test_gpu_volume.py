@@ -7,7 +7,8 @@ import numpy as np
 import pytest
 import torch
 
-from geraf_b200 import scenes, volume
+from benchkit import scenes
+from geraf_b200 import volume
 from oracle import rf_oracle as orc
 
 pytestmark = pytest.mark.gpu
@@ -48,10 +49,37 @@ def test_object_folder_build(cuda, tmp_path):
     np.testing.assert_allclose(acc.reshape(-1)[pick], total, rtol=1e-6)
 
 
-def test_sample_volume_on_gpu_matches_cpu(cuda):
+@pytest.mark.parametrize("mode,align", [("bilinear", True), ("bilinear", False), ("nearest", True)])
+def test_sample_volume_kernel_matches_the_reference_host_sampling(cuda, mode, align):
+    """The library's target-point sampling against the reference's host path
+    (torch grid_sample on the CPU, loading.py:20-25) and the FP64 restatement:
+    a ragged volume, points inside, on faces and corners, outside, and NaN."""
+    import torch.nn.functional as F
+
     rng = np.random.default_rng(1)
-    vol = torch.tensor(rng.standard_normal((9, 7, 5)).astype(np.float32))
-    pts = torch.tensor(rng.uniform(-1, 1, (100, 3)).astype(np.float32))
-    cpu = volume.sample_volume(vol, pts)
-    gpu = volume.sample_volume(vol.cuda(), pts.cuda())
-    assert torch.allclose(gpu.cpu(), cpu, atol=1e-6)
+    vol = rng.standard_normal((37, 41, 29)).astype(np.float32)
+    pts = rng.uniform(-1.15, 1.15, (20000, 3)).astype(np.float32)
+    pts[:8] = np.array([[sx, sy, sz] for sx in (-1, 1) for sy in (-1, 1) for sz in (-1, 1)], np.float32)
+    pts[8:40, 2] = 1.0
+    pts[40:44] = [[2.5, 0, 0], [0, -2.5, 0], [0, 0, 3e30], [-2.5, 2.5, 0]]
+    grid = torch.tensor(np.stack([pts[:, 2], pts[:, 1], pts[:, 0]], -1)).view(1, 1, 1, -1, 3)
+    host = F.grid_sample(torch.tensor(vol)[None, None], grid, mode=mode, align_corners=align).reshape(-1).numpy()
+    got = volume.sample_volume(torch.tensor(vol, device="cuda"), torch.tensor(pts, device="cuda"), mode,
+                               align).cpu().numpy()
+    scale = np.abs(vol).max()
+    assert np.max(np.abs(got - host)) < 1e-6 * scale
+    assert np.max(np.abs(got - orc.sample_volume(vol, pts, mode, align))) < 1e-6 * scale
+    assert np.all(got[40:44] == 0.0)
+    nan_pts = torch.tensor([[np.nan, 0.0, 0.0], [0.0, 0.0, 0.0]], device="cuda")
+    out = volume.sample_volume(torch.tensor(vol, device="cuda"), nan_pts, mode, align).cpu().numpy()
+    assert out[0] == 0.0 and np.isfinite(out[1])
+
+
+def test_sample_volume_rejects_bad_arguments(cuda):
+    vol = torch.zeros((4, 4, 4), device="cuda")
+    with pytest.raises(ValueError):
+        volume.sample_volume(vol, torch.zeros((3, 3), device="cuda"), "bicubic")
+    with pytest.raises(ValueError):
+        volume.sample_volume(vol.cpu(), torch.zeros((3, 3)))
+    empty = volume.sample_volume(torch.zeros((0, 4, 4), device="cuda"), torch.zeros((5, 3), device="cuda"))
+    assert torch.equal(empty.cpu(), torch.zeros(5))

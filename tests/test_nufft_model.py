@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import rel_l2
-from geraf_b200 import scenes
+from benchkit import scenes
 from oracle import rf_oracle as orc
 
 NODES, WEIGHTS = np.polynomial.legendre.leggauss(48)

@@ -6,7 +6,7 @@ import pytest
 import torch
 
 from conftest import rel_l2
-from geraf_b200 import scenes
+from benchkit import scenes
 from oracle import rf_oracle as orc
 from oracle import torch_tracer
 
@@ -42,6 +42,30 @@ def test_mf_peak_at_scatterer_voxel():
     yr, yi = orc.mf_forward(re, im, c["tx"], c["rx"], c["vox"], c["ch"].adc_sample_rate,
                             c["ch"].As_sci, "f64")
     assert int(np.argmax(np.hypot(yr, yi))) == 62
+
+
+@pytest.mark.parametrize("S", [16, 37, 256])
+def test_mf_rotation_form_matches_per_sample_f64(S):
+    """The FP64 rotation form used for full-size checks is the same model as the
+    per-sample libm form to ~1e-13 (forward and adjoint, S below, at and above
+    the 16-sample re-seed, antennas not a multiple of the 4 interleaved)."""
+    c = small_mf_case(S=S)
+    rng = np.random.default_rng(11)
+    A = c["re"].shape[0] - 3
+    tx, rx = c["tx"][:A], c["rx"][:A]
+    re = rng.standard_normal((A, S)).astype(np.float32)
+    im = rng.standard_normal((A, S)).astype(np.float32)
+    fs, As = c["ch"].adc_sample_rate, scenes.chirp(256).As_sci
+    exact = orc.mf_forward(re, im, tx, rx, c["vox"], fs, As, "f64")
+    rot = orc.mf_forward(re, im, tx, rx, c["vox"], fs, As, "f64r")
+    assert rel_l2(rot[0] + 1j * rot[1], exact[0] + 1j * exact[1]) < 1e-12
+    N = c["vox"].shape[1]
+    gr, gi = rng.standard_normal(N).astype(np.float32), rng.standard_normal(N).astype(np.float32)
+    exact = orc.mf_backward(gr, gi, tx, rx, c["vox"], A, S, fs, As, "f64")
+    rot = orc.mf_backward(gr, gi, tx, rx, c["vox"], A, S, fs, As, "f64r")
+    assert rel_l2(rot[0] + 1j * rot[1], exact[0] + 1j * exact[1]) < 1e-12
+    with pytest.raises(ValueError):
+        orc.mf_forward(re, im, tx, rx, c["vox"], fs, As, "f16")
 
 
 def test_mf_adjoint_identity_f64():
@@ -213,3 +237,48 @@ def test_bilinear_oracle_interpolates_and_masks():
     lhs = np.sum(gon.astype(np.float64) * on) + np.sum(gos.astype(np.float64) * os_)
     rhs = np.sum(gn.astype(np.float64) * normals) + np.sum(gs.astype(np.float64) * sig)
     assert abs(lhs - rhs) < 1e-4 * max(1.0, abs(lhs))
+
+
+def test_fd_check_machinery_against_the_fp64_adjoint():
+    """The per-ray finite-difference check used on the full-size tracer workload
+    (oracle.workload_parity.tracer_fd_errors), run here with the FP64 oracle's
+    own adjoint as the 'analytic' gradient: it must report agreement far below
+    the 1e-3 bar, and a planted error in the oracle gradient must show."""
+    from oracle import workload_parity as wp
+
+    c = tracer_case(seed=3, A=4, P=8 * 16, S=32)
+    ch = c["ch"]
+    w = dict(normals=c["normals"], sigmas=c["sigmas"], points=c["points"], tx=c["tx"], rx=c["rx"],
+             inbounds=np.ones(c["points"].shape[0], bool), S=ch.num_samples, fs=ch.adc_sample_rate,
+             f0=c["f0"], As=ch.As_sci, rays=8, samples_per_ray=16)
+    g = wp.residual(4, ch.num_samples, 5)
+    gn, gs, gp = orc.tracer_backward(g.real, g.imag, c["normals"], c["sigmas"], c["points"], c["tx"], c["rx"],
+                                     w["inbounds"], ch.adc_sample_rate, c["f0"], ch.As_sci)
+    grads = {"normals": gn, "sigmas": gs, "points": gp}
+    rays = np.arange(8)
+    errs = wp.tracer_fd_errors(grads, g, w, rays)
+    assert max(errs["sigma"], errs["normal"], errs["position"]) < 1e-6, errs
+    bad = dict(grads, points=gp * (1 + 1e-2))
+    assert wp.tracer_fd_errors(bad, g, w, rays)["position"] > 1e-3
+
+
+@pytest.mark.parametrize("mode,align", [("bilinear", True), ("bilinear", False), ("nearest", True)])
+def test_volume_sampling_restatement_matches_torch_grid_sample(mode, align):
+    """The FP64 restatement of the reference's target-point sampling against the
+    call it restates (torch grid_sample on the host, loading.py:20-25): a ragged
+    volume, points inside, on the faces and corners, and outside (zero padding)."""
+    import torch.nn.functional as F
+
+    from oracle import rf_oracle as o
+
+    rng = np.random.default_rng(2)
+    vol = rng.standard_normal((9, 7, 5)).astype(np.float32)
+    pts = rng.uniform(-1.3, 1.3, (400, 3)).astype(np.float32)
+    pts[:8] = np.array([[sx, sy, sz] for sx in (-1, 1) for sy in (-1, 1) for sz in (-1, 1)], np.float32)
+    pts[8:20, 0] = 1.0
+    pts[20:24] = [[2.5, 0, 0], [0, -2.5, 0], [0, 0, 3.0], [-2.5, 2.5, 0]]  # wholly outside
+    grid = torch.tensor(np.stack([pts[:, 2], pts[:, 1], pts[:, 0]], -1)).view(1, 1, 1, -1, 3)
+    ref = F.grid_sample(torch.tensor(vol)[None, None], grid, mode=mode, align_corners=align).reshape(-1)
+    got = o.sample_volume(vol, pts, mode, align)
+    assert np.max(np.abs(got - ref.double().numpy())) < 1e-6 * np.abs(vol).max()
+    assert np.all(got[20:24] == 0.0)

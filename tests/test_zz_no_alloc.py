@@ -13,16 +13,17 @@ import pytest
 import torch
 
 from conftest import rel_l2
-from geraf_b200 import _lib, scenes
+from benchkit import scenes
+from geraf_b200 import _lib
 
 pytestmark = pytest.mark.gpu
 
 TOL = 2e-6  # the tolerance between launch shapes of the mixed forward elsewhere in the suite
 
 
-def _case(seed, scan, S, n):
+def _case(seed, scan, S, n, n_tx=3, n_rx=4):
     rng = np.random.default_rng(seed)
-    tx, rx = scenes.virtual_array(scan)
+    tx, rx = scenes.virtual_array(scan, n_tx=n_tx, n_rx=n_rx)
     pos, amp = scenes.point_scene(rng, 6, size=0.12)
     ch = scenes.chirp(S)
     re, im = scenes.synthesize_if_numpy(tx, rx, pos, amp, ch, snr_db=20.0, rng=rng)
@@ -76,6 +77,33 @@ def test_noalloc_matches_regular_entry_point_twice_in_a_row(cuda):
         got = got_r.double().cpu().numpy() + 1j * got_i.double().cpu().numpy()
         assert np.isfinite(got).all()
         assert rel_l2(got, ref) < TOL, (seed, rel_l2(got, ref))
+
+
+def test_noalloc_with_fewer_antennas_than_one_stage(cuda):
+    """4 antennas fill less than one 8-antenna stage, so the second of the two
+    forced partial sums covers no antenna and must contribute exactly zero."""
+    t, ch = _case(2, 1, 48, 7, n_tx=1, n_rx=4)
+    assert t["re"].shape[0] == 4
+    ref_r, ref_i = _regular(t, ch)
+    got_r, got_i = _noalloc(t, ch)
+    torch.cuda.synchronize()
+    ref = ref_r.double().cpu().numpy() + 1j * ref_i.double().cpu().numpy()
+    got = got_r.double().cpu().numpy() + 1j * got_i.double().cpu().numpy()
+    assert np.isfinite(got).all()
+    assert rel_l2(got, ref) < TOL
+
+
+def test_noalloc_without_antennas_matches_regular_nan(cuda):
+    """No antennas: the reference divides a zero sum by zero antennas, so both
+    entry points write NaN."""
+    t, ch = _case(3, 2, 32, 5)
+    t = dict(t, re=t["re"][:0].contiguous(), im=t["im"][:0].contiguous(), tx=t["tx"][:0].contiguous(),
+             rx=t["rx"][:0].contiguous())
+    ref_r, ref_i = _regular(t, ch)
+    got_r, got_i = _noalloc(t, ch)
+    torch.cuda.synchronize()
+    assert torch.isnan(ref_r).all() and torch.isnan(ref_i).all()
+    assert torch.isnan(got_r).all() and torch.isnan(got_i).all()
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(cuda):
