@@ -512,18 +512,56 @@ def _ragged_extra(args, dev) -> dict:
 
     w = ragged_workload(dev, args.seed)
     ch = scenes.chirp(w["S"])
+    cfg = ch.radar_cfg(fc_start=770.0)
     vox = torch.tensor(scenes.voxel_grid(64, size=0.32).T.copy(), device=dev)
-    step = RaggedRFStep(w["normals"], w["sigmas"], w["points"], w["point_offsets"], w["tx"], w["rx"], vox,
-                        torch.full((vox.shape[0],), 1e-4, device=dev), ch.radar_cfg(fc_start=770.0))
+    A, S, P = w["tx"].shape[0], w["S"], w["P"]
+
+    def make_step():
+        return RaggedRFStep(w["normals"], w["sigmas"], w["points"], w["point_offsets"], w["tx"], w["rx"], vox,
+                            torch.full((vox.shape[0],), 1e-4, device=dev), cfg)
+
+    tuned = {}
+    if not args.no_tune:
+        # the batched tracer's forward and adjoint launch shapes, timed on the step's own inputs
+        from geraf_b200 import _lib
+        from geraf_b200.ops.RFSignalTracer.ragged import signal_tracer_ragged
+
+        nrm = w["normals"].detach().clone().requires_grad_(True)
+        g = torch.Generator(device=dev).manual_seed(args.seed + 9)
+        gx = (torch.randn((A, S), device=dev, generator=g), torch.randn((A, S), device=dev, generator=g))
+
+        def fwd(t=None):
+            return signal_tracer_ragged(nrm, w["sigmas"], w["points"], w["point_offsets"], w["tx"], w["rx"], S,
+                                        cfg["adcSampleRate"], cfg["fc_start"], cfg["As_sci"], tuning=t)
+
+        # the adjoint is timed together with the (already tuned) forward that produces its graph
+        default_f = autotune.time_call(lambda: fwd(), iters=3, warmup=1)
+        best_f, res_f = autotune.tune("tracer_ragged_forward", (A, S, P), _lib.MODE_MIXED, fwd,
+                                      autotune.ragged_forward_candidates(), iters=3)
+
+        def run_bwd(t):
+            xr, xi = signal_tracer_ragged(nrm, w["sigmas"], w["points"], w["point_offsets"], w["tx"], w["rx"],
+                                          S, cfg["adcSampleRate"], cfg["fc_start"], cfg["As_sci"],
+                                          tuning_backward=t)
+            torch.autograd.backward([xr, xi], [gx[0], gx[1]])
+
+        default_b = autotune.time_call(lambda: run_bwd(None), iters=3, warmup=1)
+        best_b, res_b = autotune.tune("tracer_ragged_backward", (A, S, P), _lib.MODE_MIXED, run_bwd,
+                                      autotune.ragged_backward_candidates(), iters=3)
+        tuned = {"forward": {"launch_shape": best_f, "candidates": len(res_f),
+                             "tuned_speedup_vs_default": round(default_f / min(m for _, m in res_f), 4)},
+                 "forward_plus_adjoint": {"launch_shape": best_b, "candidates": len(res_b),
+                                          "tuned_speedup_vs_default": round(default_b / min(m for _, m in res_b),
+                                                                            4)}}
+    step = make_step()
     step.capture()
     ms = autotune.time_call(step.run, iters=3, warmup=1)
-    A = w["tx"].shape[0]
     return {"ragged_step": {
         "workload": (f"{A} antennas, rays U[512,8192] x samples U[64,192] per antenna "
-                     f"({w['rays']} rays, {w['P']} points), S={w['S']}, MF onto 64^3 voxels"),
+                     f"({w['rays']} rays, {P} points), S={S}, MF onto 64^3 voxels"),
         "ms": round(ms, 3), "rays_per_s": round(w["rays"] / (ms * 1e-3), 1),
-        "point_samples_per_s_G": round(float(w["P"]) * w["S"] / (ms * 1e-3) / 1e9, 2),
-        "graph": True}}
+        "point_samples_per_s_G": round(float(P) * S / (ms * 1e-3) / 1e9, 2),
+        "graph": True, "autotune": tuned or "not run"}}
 
 
 def _stage1_extra(args, dev) -> dict:

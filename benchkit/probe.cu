@@ -99,6 +99,55 @@ __global__ void __launch_bounds__(128) horner_probe_kernel(float* sink, int rows
   if (s == 1234.5f) sink[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the loop live
 }
 
+// The same sum evaluated by the second-order (Goertzel) recurrence on the
+// complex samples: s_n = x_n + 2 cos(theta) s_{n+1} - s_{n+2} runs on the packed
+// (re, im) pair of one voxel with a real coefficient, one sub.rn.f32x2 and one
+// fma.rn.f32x2 per voxel-sample (8 voxels per thread, samples (re, im) from
+// shared memory, no duplication).  Same flop count per row as the Horner probe.
+__global__ void __launch_bounds__(128) goertzel_probe_kernel(float* sink, int rows, float seed) {
+  constexpr int kLen = 256;
+  constexpr int kVox = 8;
+  __shared__ __align__(16) float2 xs[kLen];
+  for (int i = threadIdx.x; i < kLen; i += blockDim.x) {
+    const float v = 1.0e-3f * static_cast<float>(i % 17) - 8.0e-3f;
+    xs[i] = make_float2(v, -v);
+  }
+  __syncthreads();
+  float2 c2[kVox], acc[kVox];
+#pragma unroll
+  for (int q = 0; q < kVox; ++q) {
+    float sn, cs;
+    sincospif(seed * static_cast<float>(threadIdx.x + 1) * 1.0e-3f + 0.1f * q, &sn, &cs);
+    c2[q] = make_float2(2.0f * cs, 2.0f * cs);
+    acc[q] = make_float2(0.0f, 0.0f);
+  }
+  for (int r = 0; r < rows; ++r) {
+    float2 s1[kVox], s2[kVox];
+#pragma unroll
+    for (int q = 0; q < kVox; ++q) s1[q] = s2[q] = make_float2(0.0f, 0.0f);
+#pragma unroll 2
+    for (int n = kLen - 2; n >= 0; n -= 2) {
+      const float4 a = *reinterpret_cast<const float4*>(&xs[n]);  // (x_n, x_n+1)
+      const float2 x[2] = {make_float2(a.z, a.w), make_float2(a.x, a.y)};
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+#pragma unroll
+        for (int q = 0; q < kVox; ++q) {
+          const float2 t = geraf::fsub2(x[h], s2[q]);
+          s2[q] = s1[q];
+          s1[q] = geraf::ffma2(c2[q], s1[q], t);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kVox; ++q) acc[q] = geraf::fadd2(acc[q], geraf::fsub2(s1[q], s2[q]));
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int q = 0; q < kVox; ++q) s += acc[q].x + acc[q].y;
+  if (s == 1234.5f) sink[blockIdx.x * blockDim.x + threadIdx.x] = s;  // keeps the loop live
+}
+
 // Counts the FP32 inputs, over all 2^32 bit patterns, for which sincosf differs
 // in any bit from separate sinf and cosf calls: the PLAIN kernels rely on there
 // being none.
@@ -139,6 +188,17 @@ GERAF_EXPORT int32_t geraf_rf_horner_probe(int32_t blocks, int32_t threads, int3
     return GERAF_ERR_INVALID_ARGUMENT;
   }
   horner_probe_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(sink, rows, 0.5f);
+  return cudaGetLastError() == cudaSuccess ? GERAF_OK : GERAF_ERR_CUDA;
+}
+
+// As geraf_rf_horner_probe, for the second-order recurrence form of the same
+// sum (flops = blocks * threads * rows * 16384).
+GERAF_EXPORT int32_t geraf_rf_goertzel_probe(int32_t blocks, int32_t threads, int32_t rows,
+                                             float* sink, void* stream) {
+  if (blocks <= 0 || threads <= 0 || threads > 128 || rows <= 0 || sink == nullptr) {
+    return GERAF_ERR_INVALID_ARGUMENT;
+  }
+  goertzel_probe_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(sink, rows, 0.5f);
   return cudaGetLastError() == cudaSuccess ? GERAF_OK : GERAF_ERR_CUDA;
 }
 

@@ -22,6 +22,8 @@ SIGNATURES = {
     # blocks x threads (<= 128) threads of the MIXED forward's Horner loop over
     # `rows` rows of 256 samples x 8 voxels: blocks * threads * rows * 16384 flops
     "geraf_rf_horner_probe": (_i32, [_i32, _i32, _i32, _vp, _vp]),
+    # the same sum by the second-order (Goertzel) recurrence, same flop count
+    "geraf_rf_goertzel_probe": (_i32, [_i32, _i32, _i32, _vp, _vp]),
     # adds to *mismatches (device u64) the FP32 inputs where sincosf differs
     # from separate sinf / cosf calls in any bit (all 2^32 inputs)
     "geraf_rf_sincos_identity_check": (_i32, [_vp, _vp]),

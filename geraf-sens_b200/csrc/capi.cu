@@ -528,10 +528,15 @@ int32_t check_ragged(int64_t A, int64_t S, int64_t P, int32_t dtype) {
 }  // namespace
 
 GERAF_EXPORT int32_t geraf_tracer_ragged_workspace_bytes(int64_t A, int64_t S, int64_t P,
-                                                         int32_t dtype, size_t* bytes) {
+                                                         int32_t dtype, const geraf_tuning_t* tuning,
+                                                         size_t* bytes) {
   if (bytes == nullptr) return fail(GERAF_ERR_INVALID_ARGUMENT, "bytes is null");
   if (int32_t rc = check_ragged(A, S, P, dtype)) return rc;
-  *bytes = tracer_ragged_workspace(A, S, P);
+  RaggedArgs a{};
+  a.A = A;
+  a.S = S;
+  a.P = P;
+  *bytes = tracer_ragged_workspace(A, S, P, tracer_ragged_forward_resolve(a, to_tuning(tuning)));
   return GERAF_OK;
 }
 
@@ -540,7 +545,7 @@ GERAF_EXPORT int32_t geraf_tracer_forward_ragged(
     const void* tx_pos, const void* rx_pos, const uint8_t* inbounds, void* output_real,
     void* output_imag, int64_t num_adc_samples, float adc_sample_rate, float start_frequency,
     float chirp_slope_scaled, int64_t total_ant_size, int64_t total_point_size, int32_t dtype,
-    void* workspace, size_t workspace_bytes, void* stream) {
+    const geraf_tuning_t* tuning, void* workspace, size_t workspace_bytes, void* stream) {
   if (int32_t rc = check_ragged(total_ant_size, num_adc_samples, total_point_size, dtype)) return rc;
   if (total_ant_size > 0 && num_adc_samples > 0) {
     REQUIRE(output_real && output_imag && tx_pos && rx_pos && point_offsets,
@@ -564,8 +569,9 @@ GERAF_EXPORT int32_t geraf_tracer_forward_ragged(
   a.f0 = start_frequency;
   a.As = chirp_slope_scaled;
   a.dtype = dtype;
-  if (int32_t rc = check_workspace(tracer_ragged_workspace(a.A, a.S, a.P), workspace, workspace_bytes)) return rc;
-  return finish_launch(tracer_forward_ragged(a, workspace, static_cast<cudaStream_t>(stream)),
+  const Tuning t = tracer_ragged_forward_resolve(a, to_tuning(tuning));
+  if (int32_t rc = check_workspace(tracer_ragged_workspace(a.A, a.S, a.P, t), workspace, workspace_bytes)) return rc;
+  return finish_launch(tracer_forward_ragged(a, t, workspace, static_cast<cudaStream_t>(stream)),
                        "signal_tracer_forward_ragged launch");
 }
 
@@ -575,7 +581,7 @@ GERAF_EXPORT int32_t geraf_tracer_backward_ragged(
     const void* rx_pos, const uint8_t* inbounds, void* grad_normals, void* grad_sigmas,
     void* grad_points, int64_t num_adc_samples, float adc_sample_rate, float start_frequency,
     float chirp_slope_scaled, int64_t total_ant_size, int64_t total_point_size, int32_t dtype,
-    void* stream) {
+    const geraf_tuning_t* tuning, void* stream) {
   if (int32_t rc = check_ragged(total_ant_size, num_adc_samples, total_point_size, dtype)) return rc;
   if (total_point_size > 0) {
     REQUIRE(grad_normals && grad_sigmas && normals && sigmas && points && point_offsets && tx_pos &&
@@ -602,7 +608,8 @@ GERAF_EXPORT int32_t geraf_tracer_backward_ragged(
   a.f0 = start_frequency;
   a.As = chirp_slope_scaled;
   a.dtype = dtype;
-  return finish_launch(tracer_backward_ragged(a, static_cast<cudaStream_t>(stream)),
+  return finish_launch(tracer_backward_ragged(a, tracer_ragged_backward_resolve(a, to_tuning(tuning)),
+                                              static_cast<cudaStream_t>(stream)),
                        "signal_tracer_backward_ragged launch");
 }
 

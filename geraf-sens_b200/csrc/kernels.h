@@ -158,9 +158,15 @@ struct RaggedArgs {
   float fs, f0, As;
   int dtype;
 };
-size_t tracer_ragged_workspace(int64_t A, int64_t S, int64_t P);
-cudaError_t tracer_forward_ragged(const RaggedArgs& a, void* ws, cudaStream_t st);
-cudaError_t tracer_backward_ragged(const RaggedArgs& a, cudaStream_t st);
+// Launch shapes of the batched tracer.  Forward: threads (64, 128, 256),
+// chunk = samples per lane (8, 16, 32), items = points per thread of one work
+// item (0: from the step's size).  Adjoint: stage_rows = residual rows staged
+// per block (1..8; 0: the default of 4, fewer when the rows are long).
+Tuning tracer_ragged_forward_resolve(const RaggedArgs& a, const Tuning& req);
+Tuning tracer_ragged_backward_resolve(const RaggedArgs& a, const Tuning& req);
+size_t tracer_ragged_workspace(int64_t A, int64_t S, int64_t P, const Tuning& t);
+cudaError_t tracer_forward_ragged(const RaggedArgs& a, const Tuning& t, void* ws, cudaStream_t st);
+cudaError_t tracer_backward_ragged(const RaggedArgs& a, const Tuning& t, cudaStream_t st);
 
 struct BilinearArgs {
   const void* normals;  // fwd: [R,S,3] in; bwd: grad_output_normals [R,T,3]

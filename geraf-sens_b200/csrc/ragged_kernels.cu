@@ -452,20 +452,24 @@ __global__ void __launch_bounds__(kBwdThreads) ragged_bwd_kernel(const RgP<T> p,
 }
 
 // ---------------------------------------------------------------------------
-constexpr int kRaggedThreads = 128;  // measured: 33.1 ms per ragged step against 33.7 ms at 256
-constexpr int kRaggedK = 16;
-
 struct RaggedLayout {
   int64_t max_items;
   size_t partial_off, items_off, counter_off, total;
   int chunk;
 };
 
-RaggedLayout ragged_layout(int64_t A, int64_t S, int64_t P) {
+// Points per work item: items_per_thread x threads when tuned, else at least
+// 2048 and more for large steps (fewer partial rows); a multiple of 256.
+int ragged_chunk(int64_t P, const Tuning& t) {
+  int64_t c = t.items > 0 ? static_cast<int64_t>(t.items) * t.threads
+                          : std::max<int64_t>(2048, std::min<int64_t>(16384, P / (148 * 8 + 1)));
+  c = std::max<int64_t>(256, std::min<int64_t>(c, 1 << 20));
+  return static_cast<int>((c + 255) / 256 * 256);
+}
+
+RaggedLayout ragged_layout(int64_t A, int64_t S, int64_t P, const Tuning& t) {
   RaggedLayout l;
-  // Chunks of at least 2048 points, more for large steps (fewer partial rows).
-  l.chunk = static_cast<int>(std::max<int64_t>(2048, std::min<int64_t>(16384, P / (148 * 8 + 1))));
-  l.chunk = (l.chunk + 255) / 256 * 256;
+  l.chunk = ragged_chunk(P, t);
   l.max_items = P / l.chunk + A + 1;
   l.partial_off = 0;
   size_t off = static_cast<size_t>(l.max_items) * std::max<int64_t>(S, 1) * sizeof(float2);
@@ -479,14 +483,16 @@ RaggedLayout ragged_layout(int64_t A, int64_t S, int64_t P) {
   return l;
 }
 
-int ragged_groups(int64_t S) {
+// Sample groups of a forward block: a power of two, G * K >= S (at most 64 and
+// at most the block's threads, so every group has a lane).
+int ragged_groups(int64_t S, int K, int threads) {
   int groups = 1;
-  while (groups * kRaggedK < S && groups < 64) groups *= 2;
+  while (groups * K < S && groups < 64 && groups * 2 <= threads) groups *= 2;
   return groups;
 }
 
 template <typename T>
-RgP<T> make_rg(const RaggedArgs& a, void* ws) {
+RgP<T> make_rg(const RaggedArgs& a, const Tuning& t, void* ws) {
   RgP<T> p{};
   p.normals = static_cast<const T*>(a.normals);
   p.sigmas = static_cast<const T*>(a.sigmas);
@@ -515,7 +521,7 @@ RgP<T> make_rg(const RaggedArgs& a, void* ws) {
   p.k1 = pc.k1;
   p.b1 = pc.b1;
   if (ws != nullptr) {
-    const RaggedLayout l = ragged_layout(a.A, a.S, a.P);
+    const RaggedLayout l = ragged_layout(a.A, a.S, a.P, t);
     unsigned char* base = static_cast<unsigned char*>(ws);
     p.partial = reinterpret_cast<float2*>(base + l.partial_off);
     p.item_offsets = reinterpret_cast<int64_t*>(base + l.items_off);
@@ -523,30 +529,36 @@ RgP<T> make_rg(const RaggedArgs& a, void* ws) {
     p.max_items = l.max_items;
     p.chunk = l.chunk;
   }
-  p.groups = ragged_groups(a.S);
+  p.groups = ragged_groups(a.S, t.chunk, t.threads);
   return p;
 }
 
-template <typename T>
-cudaError_t launch_ragged_fwd(const RaggedArgs& a, void* ws, cudaStream_t st) {
-  RgP<T> p = make_rg<T>(a, ws);
-  ragged_prep_kernel<T><<<1, 1024, 0, st>>>(p);
-  cudaError_t err = cudaGetLastError();
-  if (err != cudaSuccess) return err;
-  const void* fn = reinterpret_cast<const void*>(&ragged_fwd_kernel<T, kRaggedK>);
-  const size_t smem = std::max((static_cast<size_t>(p.groups) + 1) * kRaggedThreads * sizeof(float2) +
-                                   33 * sizeof(int),
-                               static_cast<size_t>(kRaggedThreads) * kRaggedK * sizeof(float2));
-  err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+template <typename T, int K>
+cudaError_t launch_ragged_fwd_k(RgP<T>& p, int threads, cudaStream_t st) {
+  const void* fn = reinterpret_cast<const void*>(&ragged_fwd_kernel<T, K>);
+  const size_t smem = std::max((static_cast<size_t>(p.groups) + 1) * threads * sizeof(float2) + 33 * sizeof(int),
+                               static_cast<size_t>(threads) * K * sizeof(float2));
+  cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   if (err != cudaSuccess) return err;
   int per_sm = 0;
-  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kRaggedThreads, smem);
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
   if (err != cudaSuccess) return err;
   const DeviceInfo dev = current_device_info();
   const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>(static_cast<int64_t>(per_sm) * dev.sm_count,
                                                                 p.max_items));
   void* args[] = {&p};
-  err = cudaLaunchKernel(fn, dim3(static_cast<unsigned>(blocks)), dim3(kRaggedThreads), args, smem, st);
+  return cudaLaunchKernel(fn, dim3(static_cast<unsigned>(blocks)), dim3(threads), args, smem, st);
+}
+
+template <typename T>
+cudaError_t launch_ragged_fwd(const RaggedArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  RgP<T> p = make_rg<T>(a, t, ws);
+  ragged_prep_kernel<T><<<1, 1024, 0, st>>>(p);
+  cudaError_t err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  if (t.chunk == 8) err = launch_ragged_fwd_k<T, 8>(p, t.threads, st);
+  else if (t.chunk == 32) err = launch_ragged_fwd_k<T, 32>(p, t.threads, st);
+  else err = launch_ragged_fwd_k<T, 16>(p, t.threads, st);
   if (err != cudaSuccess) return err;
   const int fin = static_cast<int>(std::min<int64_t>((a.A * a.S + 255) / 256, 148 * 16));
   ragged_finish_kernel<T><<<std::max(fin, 1), 256, 0, st>>>(p);
@@ -554,10 +566,10 @@ cudaError_t launch_ragged_fwd(const RaggedArgs& a, void* ws, cudaStream_t st) {
 }
 
 template <typename T>
-cudaError_t launch_ragged_bwd(const RaggedArgs& a, cudaStream_t st) {
-  RgP<T> p = make_rg<T>(a, nullptr);
+cudaError_t launch_ragged_bwd(const RaggedArgs& a, const Tuning& t, cudaStream_t st) {
+  RgP<T> p = make_rg<T>(a, t, nullptr);
   const int ld = static_cast<int>(((std::max<int64_t>(a.S, 1) + 3) / 4) * 4);
-  const int max_rows = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(4, (48 * 1024) / (8 * ld))));
+  const int max_rows = t.stage_rows;
   const size_t smem = static_cast<size_t>(max_rows) * 2 * ld * sizeof(float);
   const bool with_points = a.grad_points != nullptr;
   const void* fn = with_points ? reinterpret_cast<const void*>(&ragged_bwd_kernel<T, true>)
@@ -572,18 +584,44 @@ cudaError_t launch_ragged_bwd(const RaggedArgs& a, cudaStream_t st) {
 
 }  // namespace
 
-size_t tracer_ragged_workspace(int64_t A, int64_t S, int64_t P) { return ragged_layout(A, S, P).total; }
-
-cudaError_t tracer_forward_ragged(const RaggedArgs& a, void* ws, cudaStream_t st) {
-  if (a.A == 0 || a.S == 0) return cudaSuccess;
-  if (a.dtype == kF64) return launch_ragged_fwd<double>(a, ws, st);
-  return launch_ragged_fwd<float>(a, ws, st);
+Tuning tracer_ragged_forward_resolve(const RaggedArgs& a, const Tuning& req) {
+  Tuning t = req;
+  // 128 threads x 16-sample chunks: 33.1 ms per ragged step against 33.7 ms at 256 threads
+  if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 128;
+  if (t.chunk != 8 && t.chunk != 16 && t.chunk != 32) t.chunk = 16;
+  // a block's sample groups must cover all S samples (S <= 1024 is checked at the boundary)
+  while (t.chunk < 32 && static_cast<int64_t>(ragged_groups(a.S, t.chunk, t.threads)) * t.chunk < a.S) {
+    t.chunk *= 2;
+  }
+  if (t.items < 0) t.items = 0;
+  t.items = std::min(t.items, 4096);
+  return t;
 }
 
-cudaError_t tracer_backward_ragged(const RaggedArgs& a, cudaStream_t st) {
+Tuning tracer_ragged_backward_resolve(const RaggedArgs& a, const Tuning& req) {
+  Tuning t = req;
+  const int64_t ld = ((std::max<int64_t>(a.S, 1) + 3) / 4) * 4;
+  // staged rows within 48 KB of shared memory
+  const int cap = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(8, (48 * 1024) / (8 * ld))));
+  if (t.stage_rows <= 0) t.stage_rows = 4;
+  t.stage_rows = std::max(1, std::min(t.stage_rows, cap));
+  return t;
+}
+
+size_t tracer_ragged_workspace(int64_t A, int64_t S, int64_t P, const Tuning& t) {
+  return ragged_layout(A, S, P, t).total;
+}
+
+cudaError_t tracer_forward_ragged(const RaggedArgs& a, const Tuning& t, void* ws, cudaStream_t st) {
+  if (a.A == 0 || a.S == 0) return cudaSuccess;
+  if (a.dtype == kF64) return launch_ragged_fwd<double>(a, t, ws, st);
+  return launch_ragged_fwd<float>(a, t, ws, st);
+}
+
+cudaError_t tracer_backward_ragged(const RaggedArgs& a, const Tuning& t, cudaStream_t st) {
   if (a.P == 0) return cudaSuccess;
-  if (a.dtype == kF64) return launch_ragged_bwd<double>(a, st);
-  return launch_ragged_bwd<float>(a, st);
+  if (a.dtype == kF64) return launch_ragged_bwd<double>(a, t, st);
+  return launch_ragged_bwd<float>(a, t, st);
 }
 
 }  // namespace geraf

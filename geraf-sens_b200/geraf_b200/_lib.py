@@ -107,16 +107,16 @@ SIGNATURES = {
         [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _u8p, _vp, _vp, _vp, _i64, _f32, _f32, _f32, _i64,
          _i64, _i32, _i32, _tp, _vp, ctypes.c_size_t, _vp],
     ),
-    "geraf_tracer_ragged_workspace_bytes": (_i32, [_i64, _i64, _i64, _i32, _szp]),
+    "geraf_tracer_ragged_workspace_bytes": (_i32, [_i64, _i64, _i64, _i32, _tp, _szp]),
     "geraf_tracer_forward_ragged": (
         _i32,
         [_vp, _vp, _vp, _vp, _vp, _vp, _u8p, _vp, _vp, _i64, _f32, _f32, _f32, _i64, _i64, _i32,
-         _vp, ctypes.c_size_t, _vp],
+         _tp, _vp, ctypes.c_size_t, _vp],
     ),
     "geraf_tracer_backward_ragged": (
         _i32,
         [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u8p, _vp, _vp, _vp, _i64, _f32, _f32, _f32, _i64,
-         _i64, _i32, _vp],
+         _i64, _i32, _tp, _vp],
     ),
     "geraf_bilinear_forward": (
         _i32, [_vp, _vp, _vp, _vp, _vp, _vp, _u8p, _i64, _i64, _i64, _i64, _i32, _vp]

@@ -119,3 +119,15 @@ def sample_major_candidates() -> list[dict]:
 
 def tracer_backward_candidates() -> list[dict]:
     return [{"threads": t, "stage_rows": r} for t in (64, 128) for r in (4, 8, 16)]
+
+
+def ragged_forward_candidates() -> list[dict]:
+    """Batched tracer forward: threads x samples-per-lane x points per thread of a work item."""
+    return [{"threads": t, "chunk": c, "items_per_thread": i}
+            for t in (64, 128, 256) for c in (8, 16) for i in (16, 32)]
+
+
+def ragged_backward_candidates() -> list[dict]:
+    """Batched tracer adjoint: residual rows staged per block."""
+    return [{"stage_rows": r} for r in (1, 2, 4, 8)]
+

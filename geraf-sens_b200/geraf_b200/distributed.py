@@ -85,6 +85,35 @@ class _ShardedMF(torch.autograd.Function):
         return (grad_r, grad_i) + (None,) * 9
 
 
+class _GatherSlabs(torch.autograd.Function):
+    """All-gather of the ranks' (real, imag) slabs into the whole volume.
+
+    Backward: this rank's slice of the incoming gradient.  That is the gradient
+    of a loss every rank computes identically from the gathered volume (the
+    replicated-loss pattern ``gather=True`` serves); the slab adjoints are then
+    summed across ranks by the matched filter's own backward all-reduce."""
+
+    @staticmethod
+    def forward(ctx, out_r, out_i, start, end, N, group):
+        world, _ = _world(group)
+        sizes = [shard_range(N, world, r) for r in range(world)]
+        width = max(e - s for s, e in sizes)
+        pad = torch.zeros((2, width), dtype=out_r.dtype, device=out_r.device)
+        pad[0, : end - start] = out_r
+        pad[1, : end - start] = out_i
+        parts = [torch.empty_like(pad) for _ in range(world)]
+        dist.all_gather(parts, pad, group=group)
+        ctx.span = (start, end)
+        full_r = torch.cat([p[0, : e - s] for p, (s, e) in zip(parts, sizes)])
+        full_i = torch.cat([p[1, : e - s] for p, (s, e) in zip(parts, sizes)])
+        return full_r, full_i
+
+    @staticmethod
+    def backward(ctx, g_r, g_i):
+        s, e = ctx.span
+        return g_r[s:e], g_i[s:e], None, None, None, None
+
+
 def sharded_matched_filter(real: torch.Tensor, image: torch.Tensor, tpos: torch.Tensor,
                            rpos: torch.Tensor, voxel: torch.Tensor, adcSampleRate: float,
                            As_sci: float, *, precision: str | None = None, group=None,
@@ -96,7 +125,9 @@ def sharded_matched_filter(real: torch.Tensor, image: torch.Tensor, tpos: torch.
     Returns this rank's slab ``(out_real, out_imag)`` and its voxel range, or
     with ``gather=True`` the whole volume on every rank (one all-gather).  The
     gradient with respect to (real, image) is the sum of all ranks' slab
-    adjoints (one all-reduce in the backward pass).
+    adjoints (one all-reduce in the backward pass).  With ``gather=True`` every
+    rank must compute the same loss from the gathered volume: the gather's
+    backward takes each rank's own slice of that loss's gradient.
     """
     world, rank = _world(group)
     N = voxel.shape[0]
@@ -107,15 +138,7 @@ def sharded_matched_filter(real: torch.Tensor, image: torch.Tensor, tpos: torch.
                                     forward_fn or _cuda_mf_forward, backward_fn or _cuda_mf_backward)
     if not gather or world == 1:
         return out_r, out_i, (start, end)
-    sizes = [shard_range(N, world, r) for r in range(world)]
-    width = max(e - s for s, e in sizes)
-    pad = torch.zeros((2, width), dtype=out_r.dtype, device=out_r.device)
-    pad[0, : end - start] = out_r.detach()
-    pad[1, : end - start] = out_i.detach()
-    parts = [torch.empty_like(pad) for _ in range(world)]
-    dist.all_gather(parts, pad, group=group)
-    full_r = torch.cat([p[0, : e - s] for p, (s, e) in zip(parts, sizes)])
-    full_i = torch.cat([p[1, : e - s] for p, (s, e) in zip(parts, sizes)])
+    full_r, full_i = _GatherSlabs.apply(out_r, out_i, start, end, N, group)
     return full_r, full_i, (0, N)
 
 

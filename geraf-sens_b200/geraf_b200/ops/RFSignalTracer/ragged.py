@@ -17,7 +17,8 @@ from torch.autograd import Function
 from torch.autograd.function import once_differentiable
 
 from ... import _lib
-from ...runtime import check_cuda_contig, device_guard, dtype_code, ptr, stream_ptr, torch_check, workspace
+from ...runtime import (check_cuda_contig, device_guard, dtype_code, ptr, stream_ptr, torch_check, tuning_ref,
+                        tuning_struct, workspace)
 
 
 def _check(normals, sigmas, points, point_offsets, tx, rx, inbounds, S):
@@ -44,7 +45,7 @@ def _check(normals, sigmas, points, point_offsets, tx, rx, inbounds, S):
 class _RaggedTracer(Function):
     @staticmethod
     def forward(ctx, normals, sigmas, points, point_offsets, antenna_t, antenna_r, inbounds,
-                numADCSample, adcSampleRate, fc_start, As_sci):
+                numADCSample, adcSampleRate, fc_start, As_sci, tuning, tuning_backward):
         normals, sigmas, points = normals.contiguous(), sigmas.contiguous(), points.contiguous()
         antenna_t, antenna_r = antenna_t.contiguous(), antenna_r.contiguous()
         point_offsets = point_offsets.contiguous()
@@ -54,17 +55,19 @@ class _RaggedTracer(Function):
         dt = dtype_code(normals, "signal_tracer_ragged", allow_half=False)
         out_r = torch.empty((A, S), dtype=normals.dtype, device=normals.device)
         out_i = torch.empty_like(out_r)
+        tun = tuning_struct("tracer_ragged_forward", (A, S, P), _lib.MODE_MIXED, tuning)
         with device_guard(normals.device):
-            nbytes = _lib.workspace_bytes("geraf_tracer_ragged_workspace_bytes", A, S, P, dt)
+            nbytes = _lib.workspace_bytes("geraf_tracer_ragged_workspace_bytes", A, S, P, dt, tuning_ref(tun))
             ws = workspace(nbytes, normals.device)
             _lib.call("geraf_tracer_forward_ragged", ptr(normals), ptr(sigmas), ptr(points),
                       ptr(point_offsets), ptr(antenna_t), ptr(antenna_r), ptr(inbounds), ptr(out_r),
                       ptr(out_i), S, float(adcSampleRate), float(fc_start), float(As_sci), A, P, dt,
-                      ptr(ws), nbytes, stream_ptr(normals.device))
+                      tuning_ref(tun), ptr(ws), nbytes, stream_ptr(normals.device))
         ctx.save_for_backward(normals, sigmas, points, point_offsets, antenna_t, antenna_r,
                               inbounds if inbounds is not None else torch.empty(0, device=normals.device))
         ctx.has_inb = inbounds is not None
         ctx.scalars = (S, float(adcSampleRate), float(fc_start), float(As_sci), A, P, dt)
+        ctx.tuning_backward = tuning_backward
         return out_r, out_i
 
     @staticmethod
@@ -77,20 +80,24 @@ class _RaggedTracer(Function):
         gn = torch.empty_like(normals)
         gs = torch.empty_like(sigmas)
         gp = torch.empty_like(points) if ctx.needs_input_grad[2] else None
+        tun = tuning_struct("tracer_ragged_backward", (A, S, P), _lib.MODE_MIXED, ctx.tuning_backward)
         with device_guard(normals.device):
             _lib.call("geraf_tracer_backward_ragged", ptr(g_r), ptr(g_i), ptr(normals), ptr(sigmas),
                       ptr(points), ptr(offsets), ptr(tx), ptr(rx), ptr(inb), ptr(gn), ptr(gs), ptr(gp),
-                      S, fs, f0, As, A, P, dt, stream_ptr(normals.device))
+                      S, fs, f0, As, A, P, dt, tuning_ref(tun), stream_ptr(normals.device))
         return (gn if ctx.needs_input_grad[0] else None, gs if ctx.needs_input_grad[1] else None,
-                gp) + (None,) * 8
+                gp) + (None,) * 10
 
 
 def signal_tracer_ragged(normals: torch.Tensor, sigmas: torch.Tensor, points: torch.Tensor,
                          point_offsets: torch.Tensor, antenna_t: torch.Tensor, antenna_r: torch.Tensor,
                          numADCSample: int, adcSampleRate: float, fc_start: float, As_sci: float,
-                         inbounds: torch.Tensor | None = None):
-    """IF [A, S] (real, imag) of every antenna from its own points."""
+                         inbounds: torch.Tensor | None = None, *, tuning: dict | None = None,
+                         tuning_backward: dict | None = None):
+    """IF [A, S] (real, imag) of every antenna from its own points.  ``tuning`` /
+    ``tuning_backward``: launch shapes of the forward and the adjoint (default:
+    the autotuner cache, else the library's)."""
     if not all(t.is_cuda for t in (normals, sigmas, points, point_offsets, antenna_t, antenna_r)):
         raise ValueError("All signal tracer inputs must be CUDA tensors.")
     return _RaggedTracer.apply(normals, sigmas, points, point_offsets, antenna_t, antenna_r, inbounds,
-                               numADCSample, adcSampleRate, fc_start, As_sci)
+                               numADCSample, adcSampleRate, fc_start, As_sci, tuning, tuning_backward)

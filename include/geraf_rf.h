@@ -223,19 +223,24 @@ int32_t geraf_tracer_backward(const void* grad_output_real, const void* grad_out
  * Replaces a loop of SignalTracer::SignalTracer_forward calls, one per antenna
  * (SignalTracer_cuda.cu:314-356): the batched entry point has no single
  * counterpart in the reference. */
+/* Launch shape (`tuning`, may be NULL): threads (64, 128, 256), chunk =
+ * samples per lane (8, 16, 32), items_per_thread = points per thread of one
+ * work item (0: sized from the step); the workspace size depends on it. */
 int32_t geraf_tracer_ragged_workspace_bytes(int64_t total_ant_size, int64_t num_adc_samples,
                                             int64_t total_point_size, int32_t dtype,
-                                            size_t* bytes);
+                                            const geraf_tuning_t* tuning, size_t* bytes);
 int32_t geraf_tracer_forward_ragged(const void* normals, const void* sigmas, const void* points,
                                     const int64_t* point_offsets, const void* tx_pos,
                                     const void* rx_pos, const uint8_t* inbounds, void* output_real,
                                     void* output_imag, int64_t num_adc_samples,
                                     float adc_sample_rate, float start_frequency,
                                     float chirp_slope_scaled, int64_t total_ant_size,
-                                    int64_t total_point_size, int32_t dtype, void* workspace,
+                                    int64_t total_point_size, int32_t dtype,
+                                    const geraf_tuning_t* tuning, void* workspace,
                                     size_t workspace_bytes, void* stream);
 /* Adjoint of geraf_tracer_forward_ragged: grad_sigmas [P], grad_normals [P,3]
  * and, when non-NULL, grad_points [P,3]; out-of-bounds points get zeros.
+ * `tuning` (may be NULL): stage_rows = residual rows staged per block (1..8). 
  * Replaces the per-antenna SignalTracer::SignalTracer_backward_normal_sigma
  * calls (SignalTracer_cuda.cu:358-406). */
 int32_t geraf_tracer_backward_ragged(const void* grad_output_real, const void* grad_output_imag,
@@ -246,7 +251,7 @@ int32_t geraf_tracer_backward_ragged(const void* grad_output_real, const void* g
                                      int64_t num_adc_samples, float adc_sample_rate,
                                      float start_frequency, float chirp_slope_scaled,
                                      int64_t total_ant_size, int64_t total_point_size,
-                                     int32_t dtype, void* stream);
+                                     int32_t dtype, const geraf_tuning_t* tuning, void* stream);
 
 /* Linear resampling along rays: for each ray and target depth, bracket the
  * target in the ray's coarse depths by binary search and interpolate sigma

@@ -97,9 +97,13 @@ def _worker(rank, world, port, outdir):
             ch.adc_sample_rate, ch.As_sci, forward_fn=oracle_mf_fwd, backward_fn=oracle_mf_bwd)
         loss = (yr * torch.tensor(c["gr"][s:e])).sum() + (yi * torch.tensor(c["gi"][s:e])).sum()
         loss.backward()
+        # the gathered volume is differentiable: the same loss on every rank from the whole volume
+        re2 = re.detach().clone().requires_grad_(True)
+        im2 = im.detach().clone().requires_grad_(True)
         full_r, full_i, _ = gd.sharded_matched_filter(
-            re.detach(), im.detach(), torch.tensor(c["tx"]), torch.tensor(c["rx"]), torch.tensor(c["vox"]),
+            re2, im2, torch.tensor(c["tx"]), torch.tensor(c["rx"]), torch.tensor(c["vox"]),
             ch.adc_sample_rate, ch.As_sci, gather=True, forward_fn=oracle_mf_fwd, backward_fn=oracle_mf_bwd)
+        ((full_r * torch.tensor(c["gr"])).sum() + (full_i * torch.tensor(c["gi"])).sum()).backward()
         # tracer, antenna-sharded
         n = torch.tensor(c["nrm"], dtype=torch.float64, requires_grad=True)
         sg = torch.tensor(c["sig"], dtype=torch.float64, requires_grad=True)
@@ -110,7 +114,8 @@ def _worker(rank, world, port, outdir):
             ch.As_sci, forward_fn=oracle_tr_fwd, backward_fn=oracle_tr_bwd)
         ((xr * torch.tensor(c["hr"][a0:a1])).sum() + (xi * torch.tensor(c["hi"][a0:a1])).sum()).backward()
         np.savez(os.path.join(outdir, f"rank{rank}.npz"), yr=_np(yr), yi=_np(yi), s=s, e=e,
-                 gre=_np(re.grad), gim=_np(im.grad), full_r=_np(full_r), full_i=_np(full_i), xr=_np(xr),
+                 gre=_np(re.grad), gim=_np(im.grad), full_r=_np(full_r), full_i=_np(full_i),
+                 gre2=_np(re2.grad), gim2=_np(im2.grad), xr=_np(xr),
                  xi=_np(xi), a0=a0, a1=a1, gn=_np(n.grad), gs=_np(sg.grad), gp=_np(p.grad))
     finally:
         dist.destroy_process_group()
@@ -161,6 +166,9 @@ def test_two_rank_gloo_matches_unsharded(tmp_path):
         # the all-reduced slab adjoints equal the unsharded adjoint on every rank
         np.testing.assert_allclose(d["gre"], ref_gr, rtol=1e-6, atol=1e-9)
         np.testing.assert_allclose(d["gim"], ref_gi, rtol=1e-6, atol=1e-9)
+        # and through the gathered volume
+        np.testing.assert_allclose(d["gre2"], ref_gr, rtol=1e-6, atol=1e-9)
+        np.testing.assert_allclose(d["gim2"], ref_gi, rtol=1e-6, atol=1e-9)
         a0, a1 = int(d["a0"]), int(d["a1"])
         np.testing.assert_allclose(d["xr"], tr_r[a0:a1], rtol=1e-6, atol=1e-12)
         np.testing.assert_allclose(d["xi"], tr_i[a0:a1], rtol=1e-6, atol=1e-12)

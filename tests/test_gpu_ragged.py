@@ -181,3 +181,37 @@ def test_adjoint_with_tiles_spanning_many_antennas(cuda):
         assert rel_l2(sig.grad[s:e].double().cpu().numpy(), gs[0]) < MIXED_TOL, a
         assert rel_l2(nrm.grad[s:e].double().cpu().numpy(), gn) < MIXED_TOL, a
         assert rel_l2(pts.grad[s:e].double().cpu().numpy(), gp) < MIXED_TOL, a
+
+
+@pytest.mark.parametrize("fwd_tuning,bwd_tuning", [
+    ({"threads": 64, "chunk": 8, "items_per_thread": 4}, {"stage_rows": 1}),
+    ({"threads": 256, "chunk": 32, "items_per_thread": 16}, {"stage_rows": 8}),
+    ({"threads": 128, "chunk": 8}, {"stage_rows": 2}),
+])
+def test_launch_shapes_agree(cuda, fwd_tuning, bwd_tuning):
+    """Every tuned launch shape gives the library default's results (sums in
+    other orders only) for the forward and the adjoint, S above one block's
+    8-sample-chunk reach included."""
+    from geraf_b200.ops.RFSignalTracer.ragged import signal_tracer_ragged
+
+    for S in (48, 600):
+        c = ragged_case(seed=6, A=6, S=S, counts=[1500, 1, 2600, 0, 700, 3100])
+        ch = c["ch"]
+        outs = []
+        for ft, bt in ((None, None), (fwd_tuning, bwd_tuning)):
+            t = {k: torch.tensor(c[k], device="cuda") for k in ("tx", "rx", "pts", "nrm", "sig", "off")}
+            for k in ("pts", "nrm", "sig"):
+                t[k].requires_grad_(True)
+            xr, xi = signal_tracer_ragged(t["nrm"], t["sig"], t["pts"], t["off"], t["tx"], t["rx"], S,
+                                          ch.adc_sample_rate, c["f0"], ch.As_sci,
+                                          inbounds=torch.tensor(c["inb"], device="cuda"), tuning=ft,
+                                          tuning_backward=bt)
+            g = torch.Generator(device="cuda").manual_seed(1)
+            gr = torch.randn(xr.shape, device="cuda", generator=g)
+            gi = torch.randn(xr.shape, device="cuda", generator=g)
+            keep = torch.isfinite(xr[:, 0])  # antenna 3 has no points: 0/0
+            ((xr[keep] * gr[keep]).sum() + (xi[keep] * gi[keep]).sum()).backward()
+            outs.append([torch.complex(xr, xi)[keep].cpu().numpy()] +
+                        [t[k].grad.double().cpu().numpy() for k in ("sig", "nrm", "pts")])
+        for a, b in zip(outs[0], outs[1]):
+            assert rel_l2(b, a) < 2e-6
