@@ -360,11 +360,14 @@ GERAF_EXPORT int32_t geraf_mf_fft_forward(const void* real, const void* imag, co
                                           const void* voxel, int64_t total_ant_size,
                                           int64_t num_range_bins, float fft_spacing,
                                           float adc_sample_rate, float chirp_slope_scaled,
-                                          int64_t num_voxels, int32_t dtype, void* stream) {
+                                          int64_t num_voxels, int32_t dtype, int32_t flags,
+                                          void* stream) {
   (void)adc_sample_rate;
   (void)chirp_slope_scaled;
   if (int32_t rc = check_mf_sizes(total_ant_size, num_range_bins, num_voxels, dtype, GERAF_MODE_PLAIN)) return rc;
+  REQUIRE((flags & ~GERAF_FFT_CONSISTENT_BINS) == 0, "unknown range-bin flags");
   MfFftArgs a{};
+  a.consistent_bins = (flags & GERAF_FFT_CONSISTENT_BINS) != 0;
   a.real = real;
   a.imag = imag;
   a.tx = tx_pos;
@@ -387,13 +390,16 @@ GERAF_EXPORT int32_t geraf_mf_fft_backward(const void* grad_output_real, const v
                                            const void* voxel, int64_t total_ant_size,
                                            int64_t num_range_bins, float fft_spacing,
                                            float adc_sample_rate, float chirp_slope_scaled,
-                                           int64_t num_voxels, int32_t dtype, void* stream) {
+                                           int64_t num_voxels, int32_t dtype, int32_t flags,
+                                           void* stream) {
   (void)real;
   (void)imag;
   (void)adc_sample_rate;
   (void)chirp_slope_scaled;
   if (int32_t rc = check_mf_sizes(total_ant_size, num_range_bins, num_voxels, dtype, GERAF_MODE_PLAIN)) return rc;
+  REQUIRE((flags & ~GERAF_FFT_CONSISTENT_BINS) == 0, "unknown range-bin flags");
   MfFftArgs a{};
+  a.consistent_bins = (flags & GERAF_FFT_CONSISTENT_BINS) != 0;
   a.tx = tx_pos;
   a.rx = rx_pos;
   a.out_real = grad_real;

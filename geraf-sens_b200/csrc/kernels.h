@@ -92,6 +92,10 @@ struct MfFftArgs {
   int64_t A, bins, N;
   float spacing;
   int dtype;
+  // false: the reference's bound (a delay d is kept when d <= spacing * bins, though
+  // its bin floor(d / spacing / 2) reaches only half the bins); true: the bound
+  // matches the index (d <= 2 spacing bins), so every bin can be reached
+  bool consistent_bins;
 };
 cudaError_t mf_fft_forward(const MfFftArgs& a, cudaStream_t st);
 cudaError_t mf_fft_backward(const MfFftArgs& a, cudaStream_t st);

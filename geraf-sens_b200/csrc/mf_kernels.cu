@@ -537,7 +537,16 @@ struct MfFftP {
   T* out_i;
   int64_t A, bins, N;
   float spacing;
+  int consistent_bins;
 };
+
+// Largest path delay kept by the range-bin kernels: the reference's
+// spacing * bins (MatchedFilter_cuda_kernel.cu:143-148), or twice that when the
+// bound is made consistent with the bin index floor(d / spacing / 2).
+template <typename T>
+__device__ __forceinline__ float fft_bound(const MfFftP<T>& p, int num_range_bins) {
+  return p.consistent_bins ? 2.0f * (p.spacing * num_range_bins) : p.spacing * num_range_bins;
+}
 
 template <typename T>
 __global__ void __launch_bounds__(256) mf_fft_fwd_kernel(const MfFftP<T> p) {
@@ -552,7 +561,7 @@ __global__ void __launch_bounds__(256) mf_fft_fwd_kernel(const MfFftP<T> p) {
     const float tx_distance = sqrtf(sq(tx_x - vx) + sq(tx_y - vy) + sq(tx_z - vz));
     const float rx_distance = sqrtf(sq(rx_x - vx) + sq(rx_y - vy) + sq(rx_z - vz));
     const float distance = tx_distance + rx_distance + kPathBias;
-    if (distance < 0.0f || distance > p.spacing * num_range_bins) continue;
+    if (distance < 0.0f || distance > fft_bound(p, num_range_bins)) continue;
     const int range_bin = static_cast<int>(floorf(distance / p.spacing / 2.0f));
     if (range_bin < 0 || range_bin >= num_range_bins) continue;
     const float tau = distance / kSpeedOfLight;
@@ -593,7 +602,7 @@ __global__ void __launch_bounds__(128) mf_fft_bwd_kernel(const MfFftP<T> p) {
       const float rx_distance = sqrtf(sq(rx_x - vx) + sq(rx_y - vy) + sq(rx_z - vz));
       const float distance = tx_distance + rx_distance + kPathBias;
       int bin = -1;
-      if (!(distance < 0.0f || distance > p.spacing * num_range_bins)) {
+      if (!(distance < 0.0f || distance > fft_bound(p, num_range_bins))) {
         bin = static_cast<int>(floorf(distance / p.spacing / 2.0f));
       }
       s_bin[i] = bin;
@@ -836,6 +845,7 @@ cudaError_t launch_fft(const MfFftArgs& a, bool backward, cudaStream_t st) {
   p.bins = a.bins;
   p.N = a.N;
   p.spacing = a.spacing;
+  p.consistent_bins = a.consistent_bins ? 1 : 0;
   if (!backward) {
     const int64_t blocks = (a.N + 255) / 256;
     mf_fft_fwd_kernel<T><<<static_cast<unsigned>(blocks), 256, 0, st>>>(p);

@@ -32,6 +32,8 @@ MODE_NUFFT = 2
 SAMPLE_TRILINEAR = 0
 SAMPLE_NEAREST = 1
 
+FFT_CONSISTENT_BINS = 1
+
 
 class Tuning(ctypes.Structure):
     """``geraf_tuning_t``: launch shape; 0 in any field = library default."""
@@ -86,12 +88,12 @@ SIGNATURES = {
          _tp, _vp, ctypes.c_size_t, _vp],
     ),
     "geraf_mf_fft_forward": (
-        _i32, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _f32, _f32, _f32, _i64, _i32, _vp]
+        _i32, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _f32, _f32, _f32, _i64, _i32, _i32, _vp]
     ),
     "geraf_mf_fft_backward": (
         _i32,
         [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _f32, _f32, _f32, _i64, _i32,
-         _vp],
+         _i32, _vp],
     ),
     "geraf_tracer_forward_workspace_bytes": (_i32, [_i64, _i64, _i64, _i32, _i32, _tp, _szp]),
     "geraf_tracer_forward": (

@@ -137,32 +137,40 @@ def MatchedFilter_backward_realimag(grad_output_real, grad_output_imag, real, im
 
 def MatchedFilter_fft_forward(real, imag, tx_pos, rx_pos, output_real, output_imag, voxel,
                               total_ant_size, num_range_bins, fft_spacing, adc_sample_rate,
-                              chirp_slope_scaled, num_voxels):
-    """Range-bin matched filter (reference: MatchedFilter_cuda_kernel.cu:117-169)."""
+                              chirp_slope_scaled, num_voxels, *, consistent_bins=False):
+    """Range-bin matched filter (reference: MatchedFilter_cuda_kernel.cu:117-169).
+
+    ``consistent_bins=True`` keeps path delays up to 2 * fft_spacing * bins, the
+    bound that matches the bin index floor(d / fft_spacing / 2); the default is
+    the reference's bound fft_spacing * bins (:143-148), which reaches only the
+    first half of the bins."""
     A, B, N = int(total_ant_size), int(num_range_bins), int(num_voxels)
     _check_forward(real, imag, tx_pos, rx_pos, output_real, output_imag, voxel, A, B, N)
     dt = dtype_code(real, "matched_filter_fft_forward_cuda", allow_half=True)
+    flags = _lib.FFT_CONSISTENT_BINS if consistent_bins else 0
     with device_guard(real.device):
         _lib.call("geraf_mf_fft_forward", ptr(real), ptr(imag), ptr(tx_pos), ptr(rx_pos),
                   ptr(output_real), ptr(output_imag), ptr(voxel), A, B, float(fft_spacing),
-                  float(adc_sample_rate), float(chirp_slope_scaled), N, dt,
+                  float(adc_sample_rate), float(chirp_slope_scaled), N, dt, flags,
                   stream_ptr(real.device))
 
 
 def MatchedFilter_fft_backward_realimag(grad_output_real, grad_output_imag, real, imag, tx_pos,
                                         rx_pos, grad_real, grad_imag, voxel, total_ant_size,
                                         num_range_bins, fft_spacing, adc_sample_rate,
-                                        chirp_slope_scaled, num_voxels):
-    """Adjoint of :func:`MatchedFilter_fft_forward` (MatchedFilter_cuda_kernel.cu:222-279)."""
+                                        chirp_slope_scaled, num_voxels, *, consistent_bins=False):
+    """Adjoint of :func:`MatchedFilter_fft_forward` (MatchedFilter_cuda_kernel.cu:222-279),
+    with the same ``consistent_bins``."""
     A, B, N = int(total_ant_size), int(num_range_bins), int(num_voxels)
     _check_backward(grad_output_real, grad_output_imag, real, imag, tx_pos, rx_pos, grad_real,
                     grad_imag, voxel, A, B, N)
     dt = dtype_code(real, "matched_filter_fft_backward_realimag_cuda", allow_half=True)
+    flags = _lib.FFT_CONSISTENT_BINS if consistent_bins else 0
     with device_guard(real.device):
         _lib.call("geraf_mf_fft_backward", ptr(grad_output_real), ptr(grad_output_imag),
                   ptr(real), ptr(imag), ptr(tx_pos), ptr(rx_pos), ptr(grad_real), ptr(grad_imag),
                   ptr(voxel), A, B, float(fft_spacing), float(adc_sample_rate),
-                  float(chirp_slope_scaled), N, dt, stream_ptr(real.device))
+                  float(chirp_slope_scaled), N, dt, flags, stream_ptr(real.device))
 
 
 def get_cuda_version() -> str:

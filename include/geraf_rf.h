@@ -133,14 +133,18 @@ int32_t geraf_mf_backward(const void* grad_output_real, const void* grad_output_
 
 /* Range-bin variant: per antenna, gather bin floor(d/fft_spacing/2) of the
  * [A,bins] spectrum (skipped when d > fft_spacing*bins) times exp(-j 2 pi 773.704 tau).
+ * `flags`: 0 for the reference's behaviour; GERAF_FFT_CONSISTENT_BINS keeps
+ * delays up to 2*fft_spacing*bins instead, the bound that matches the bin index
+ * (the reference's bound reaches only the first half of the bins).
  * Replaces MatchedFilter::MatchedFilter_fft_forward (MatchedFilter_cuda.cu:212-251,
  * kernel MatchedFilter_cuda_kernel.cu:117-169). */
+#define GERAF_FFT_CONSISTENT_BINS 1
 int32_t geraf_mf_fft_forward(const void* real, const void* imag, const void* tx_pos,
                              const void* rx_pos, void* output_real, void* output_imag,
                              const void* voxel, int64_t total_ant_size, int64_t num_range_bins,
                              float fft_spacing, float adc_sample_rate, float chirp_slope_scaled,
-                             int64_t num_voxels, int32_t dtype, void* stream);
-/* Adjoint of geraf_mf_fft_forward.  Replaces
+                             int64_t num_voxels, int32_t dtype, int32_t flags, void* stream);
+/* Adjoint of geraf_mf_fft_forward (same `flags`).  Replaces
  * MatchedFilter::MatchedFilter_fft_backward_realimag (MatchedFilter_cuda.cu:299-343,
  * kernel MatchedFilter_cuda_kernel.cu:222-279). */
 int32_t geraf_mf_fft_backward(const void* grad_output_real, const void* grad_output_imag,
@@ -148,7 +152,7 @@ int32_t geraf_mf_fft_backward(const void* grad_output_real, const void* grad_out
                               const void* rx_pos, void* grad_real, void* grad_imag,
                               const void* voxel, int64_t total_ant_size, int64_t num_range_bins,
                               float fft_spacing, float adc_sample_rate, float chirp_slope_scaled,
-                              int64_t num_voxels, int32_t dtype, void* stream);
+                              int64_t num_voxels, int32_t dtype, int32_t flags, void* stream);
 
 /* Matched-filter forward (MIXED form, FP32 arrays) that allocates nothing and
  * takes no workspace.  No counterpart in the reference.  It serves callers that

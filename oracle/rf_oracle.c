@@ -240,16 +240,19 @@ void oracle_mf_backward_f64r(const float* gr, const float* gi, const float* tx, 
 
 /* Range-bin variants: FP32 reference order only (the bin index is a
  * floor of an FP32 quotient, so an FP64 form would bin differently). */
+/* consistent != 0: keep delays up to 2 * spacing * bins, the bound that matches
+ * the bin index (the reference keeps only d <= spacing * bins). */
 void oracle_mf_fft_forward_f32(const float* re, const float* im, const float* tx, const float* rx,
                                const float* vox, int64_t A, int64_t B, int64_t N, float spacing,
-                               float* out_re, float* out_im) {
+                               int consistent, float* out_re, float* out_im) {
   const int bins = (int)B;
+  const float bound = consistent ? 2.0f * (spacing * bins) : spacing * bins;
 #pragma omp parallel for schedule(dynamic, 16)
   for (int64_t v = 0; v < N; ++v) {
     float ar = 0.0f, ai = 0.0f;
     for (int64_t a = 0; a < A; ++a) {
       const float distance = mf_distance_f32(tx, rx, a, vox[v], vox[N + v], vox[2 * N + v]);
-      if (distance < 0.0f || distance > spacing * bins) continue;
+      if (distance < 0.0f || distance > bound) continue;
       const int bin = (int)floorf(distance / spacing / 2.0f);
       if (bin < 0 || bin >= bins) continue;
       const float tau = distance / K_C;
@@ -266,15 +269,16 @@ void oracle_mf_fft_forward_f32(const float* re, const float* im, const float* tx
 
 void oracle_mf_fft_backward_f32(const float* gr, const float* gi, const float* tx, const float* rx,
                                 const float* vox, int64_t A, int64_t B, int64_t N, float spacing,
-                                float* grad_re, float* grad_im) {
+                                int consistent, float* grad_re, float* grad_im) {
   const int bins = (int)B;
+  const float bound = consistent ? 2.0f * (spacing * bins) : spacing * bins;
 #pragma omp parallel for schedule(dynamic, 1)
   for (int64_t a = 0; a < A; ++a) {
     for (int64_t b = 0; b < B; ++b) {
       float ar = 0.0f, ai = 0.0f;
       for (int64_t v = 0; v < N; ++v) {
         const float distance = mf_distance_f32(tx, rx, a, vox[v], vox[N + v], vox[2 * N + v]);
-        if (distance < 0.0f || distance > spacing * bins) continue;
+        if (distance < 0.0f || distance > bound) continue;
         const int vb = (int)floorf(distance / spacing / 2.0f);
         if (vb != (int)b) continue;
         const float tau = distance / K_C;

@@ -47,7 +47,7 @@ def lib():
         L.oracle_mf_backward_f32.argtypes = mf + [_f32p, _f32p]
         L.oracle_mf_forward_f64r.argtypes = mf + [_f64p, _f64p]
         L.oracle_mf_backward_f64r.argtypes = mf + [_f64p, _f64p]
-        fft = [_f32p, _f32p, _f32p, _f32p, _f32p, _i64, _i64, _i64, _f, _f32p, _f32p]
+        fft = [_f32p, _f32p, _f32p, _f32p, _f32p, _i64, _i64, _i64, _f, ctypes.c_int, _f32p, _f32p]
         L.oracle_mf_fft_forward_f32.argtypes = fft
         L.oracle_mf_fft_backward_f32.argtypes = fft
         tr = [_f32p, _f32p, _f32p, _f32p, _f32p, _u8p, _i64, _i64, _i64, _f, _f, _f]
@@ -112,22 +112,27 @@ def mf_backward(grad_r, grad_i, tx, rx, voxel_3n, A, S, fs, As, form="f64"):
     return out_r, out_i
 
 
-def mf_fft_forward(real, imag, tx, rx, voxel_3n, spacing):
+def mf_fft_forward(real, imag, tx, rx, voxel_3n, spacing, consistent_bins=False):
+    """Range-bin forward (MatchedFilter_cuda_kernel.cu:117-169); ``consistent_bins``
+    keeps delays up to 2 * spacing * bins instead of the reference's spacing * bins."""
     real, imag, tx, rx, vox = map(_f32, (real, imag, tx, rx, voxel_3n))
     A, B = real.shape
     N = vox.shape[1]
     out_r = np.zeros(N, np.float32)
     out_i = np.zeros(N, np.float32)
-    lib().oracle_mf_fft_forward_f32(real, imag, tx, rx, vox, A, B, N, spacing, out_r, out_i)
+    lib().oracle_mf_fft_forward_f32(real, imag, tx, rx, vox, A, B, N, spacing, int(consistent_bins), out_r,
+                                    out_i)
     return out_r, out_i
 
 
-def mf_fft_backward(grad_r, grad_i, tx, rx, voxel_3n, A, B, spacing):
+def mf_fft_backward(grad_r, grad_i, tx, rx, voxel_3n, A, B, spacing, consistent_bins=False):
+    """Range-bin adjoint (MatchedFilter_cuda_kernel.cu:222-279)."""
     gr, gi, tx, rx, vox = map(_f32, (grad_r, grad_i, tx, rx, voxel_3n))
     N = vox.shape[1]
     out_r = np.zeros((A, B), np.float32)
     out_i = np.zeros((A, B), np.float32)
-    lib().oracle_mf_fft_backward_f32(gr, gi, tx, rx, vox, A, B, N, spacing, out_r, out_i)
+    lib().oracle_mf_fft_backward_f32(gr, gi, tx, rx, vox, A, B, N, spacing, int(consistent_bins), out_r,
+                                     out_i)
     return out_r, out_i
 
 

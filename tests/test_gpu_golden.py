@@ -12,6 +12,7 @@ import torch
 
 from conftest import rel_l2
 from gpu_helpers import cu, golden_cases, load_golden, mf_backward, mf_forward, tracer_backward, tracer_forward
+from oracle import rf_oracle as orc
 
 pytestmark = pytest.mark.gpu
 
@@ -150,3 +151,36 @@ def test_bilinear_matches_reference_bitwise(cuda, name):
                                   cu(g["z_vals"]), cu(g["tgt_z_vals"]), gn, gs, A, R, S, T)
     np.testing.assert_array_equal(gn.cpu().numpy(), g["grad_normals"])
     np.testing.assert_array_equal(gs.cpu().numpy(), g["grad_sigmas"])
+
+
+@pytest.mark.parametrize("consistent", [False, True])
+def test_mf_fft_consistent_bins_flag(cuda, consistent):
+    """The range-bin kernels with the bound made consistent with the bin index
+    (an opt-in fix of MatchedFilter_cuda_kernel.cu:143-148) against the FP32
+    oracle with the same bound; the default stays the reference's."""
+    from geraf_b200.ops.RFMatchedFilter import _C
+
+    g = load_golden("mf_fft_f32")
+    A, B = g["spec_real"].shape
+    N = g["voxel"].shape[1]
+    spacing = 0.02
+    args = [cu(g[k]) for k in ("spec_real", "spec_imag", "tx", "rx")]
+    out_r = torch.full((N,), float("nan"), device="cuda")
+    out_i = torch.full((N,), float("nan"), device="cuda")
+    _C.MatchedFilter_fft_forward(*args, out_r, out_i, cu(g["voxel"]), A, B, spacing, float(g["fs"]),
+                                 float(g["As"]), N, consistent_bins=consistent)
+    h_r = torch.full((A, B), float("nan"), device="cuda")
+    h_i = torch.full((A, B), float("nan"), device="cuda")
+    _C.MatchedFilter_fft_backward_realimag(cu(g["grad_output_real"]), cu(g["grad_output_imag"]), *args, h_r, h_i,
+                                           cu(g["voxel"]), A, B, spacing, float(g["fs"]), float(g["As"]), N,
+                                           consistent_bins=consistent)
+    torch.cuda.synchronize()
+    rr, ri = orc.mf_fft_forward(g["spec_real"], g["spec_imag"], g["tx"], g["rx"], g["voxel"], spacing, consistent)
+    hr, hi = orc.mf_fft_backward(g["grad_output_real"], g["grad_output_imag"], g["tx"], g["rx"], g["voxel"], A,
+                                 B, spacing, consistent)
+    got = out_r.cpu().numpy() + 1j * out_i.cpu().numpy()
+    # the scene's delays (~0.95 m) lie between the two bounds (0.8 and 1.6 m)
+    assert (np.count_nonzero(got) > 0) == consistent
+    assert rel_l2(got, rr + 1j * ri) < 1e-5
+    assert rel_l2(h_r.cpu().numpy() + 1j * h_i.cpu().numpy(), hr + 1j * hi) < 1e-5
+

@@ -104,7 +104,8 @@ def test_mf_f32_tracks_f64():
     assert rel_l2(b32[0] + 1j * b32[1], b64[0] + 1j * b64[1]) < 5e-4
 
 
-def test_mf_fft_adjoint_identity_f32():
+@pytest.mark.parametrize("consistent", [False, True])
+def test_mf_fft_adjoint_identity_f32(consistent):
     c = small_mf_case()
     rng = np.random.default_rng(5)
     A, B = c["tx"].shape[0], 40
@@ -112,12 +113,29 @@ def test_mf_fft_adjoint_identity_f32():
     sr, si = rng.standard_normal((A, B)).astype(np.float32), rng.standard_normal((A, B)).astype(np.float32)
     gr, gi = rng.standard_normal(N).astype(np.float32), rng.standard_normal(N).astype(np.float32)
     spacing = 0.03
-    yr, yi = orc.mf_fft_forward(sr, si, c["tx"], c["rx"], c["vox"], spacing)
-    hr, hi = orc.mf_fft_backward(gr, gi, c["tx"], c["rx"], c["vox"], A, B, spacing)
+    yr, yi = orc.mf_fft_forward(sr, si, c["tx"], c["rx"], c["vox"], spacing, consistent)
+    hr, hi = orc.mf_fft_backward(gr, gi, c["tx"], c["rx"], c["vox"], A, B, spacing, consistent)
     lhs = np.dot(gr.astype(np.float64), yr) + np.dot(gi.astype(np.float64), yi)
     rhs = np.sum(hr.astype(np.float64) * sr) + np.sum(hi.astype(np.float64) * si)
     assert np.count_nonzero(hr) > 0
     assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), 1.0)
+
+
+def test_mf_fft_consistent_bins_reach_the_upper_half():
+    """The reference keeps delays d <= spacing * bins although the bin index
+    floor(d / spacing / 2) then reaches only bins [0, bins/2]; with the consistent
+    bound the upper bins are filled and the lower ones are unchanged."""
+    c = small_mf_case()
+    A, N = c["tx"].shape[0], c["vox"].shape[1]
+    rng = np.random.default_rng(6)
+    gr, gi = rng.standard_normal(N).astype(np.float32), rng.standard_normal(N).astype(np.float32)
+    spacing, B = 0.02, 64      # delays ~0.95 m: bins ~24, past the reference's bound 1.28 m / 2
+    ref_r, _ = orc.mf_fft_backward(gr, gi, c["tx"], c["rx"], c["vox"], A, B, spacing, False)
+    fix_r, _ = orc.mf_fft_backward(gr, gi, c["tx"], c["rx"], c["vox"], A, B, spacing, True)
+    assert np.count_nonzero(ref_r[:, B // 2:]) == 0
+    assert np.count_nonzero(fix_r) > 0
+    both = ref_r != 0
+    assert np.array_equal(fix_r[both], ref_r[both])
 
 
 def tracer_case(seed=0, A=5, P=300, S=24):
