@@ -20,10 +20,13 @@
 namespace geraf {
 namespace {
 
-// grid_sample's unnormalisation of coordinate c in [-1, 1] to a source index.
+// grid_sample's unnormalisation of coordinate c in [-1, 1] to a source index,
+// ((c + 1) / 2) (size - 1) or ((c + 1) size - 1) / 2, each operation rounded on
+// its own (no fused multiply-add) as torch's host code rounds it.
 __device__ __forceinline__ float source_index(float c, int size, bool align) {
-  return align ? (c + 1.0f) * 0.5f * static_cast<float>(size - 1)
-               : ((c + 1.0f) * static_cast<float>(size) - 1.0f) * 0.5f;
+  const float c1 = __fadd_rn(c, 1.0f);
+  return align ? __fmul_rn(__fmul_rn(c1, 0.5f), static_cast<float>(size - 1))
+               : __fmul_rn(__fsub_rn(__fmul_rn(c1, static_cast<float>(size)), 1.0f), 0.5f);
 }
 
 __global__ void __launch_bounds__(256) volume_sample_kernel(const float* __restrict__ vol, int nx,

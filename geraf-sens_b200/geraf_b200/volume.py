@@ -59,10 +59,13 @@ def build_mf_volume(adc_real, adc_imag, tpos, rpos, adc_sample_rate: float, As_s
     from .ops.RFMatchedFilter import _C
 
     dev = torch.device(device)
-    re = torch.as_tensor(np.asarray(adc_real, np.float32)).to(dev).contiguous()
-    im = torch.as_tensor(np.asarray(adc_imag, np.float32)).to(dev).contiguous()
-    tx = torch.as_tensor(np.asarray(tpos, np.float32).reshape(-1, 3)).to(dev).contiguous()
-    rx = torch.as_tensor(np.asarray(rpos, np.float32).reshape(-1, 3)).to(dev).contiguous()
+
+    def dev_f32(x):  # numpy arrays or tensors on any device
+        t = x if isinstance(x, torch.Tensor) else torch.as_tensor(np.asarray(x, np.float32))
+        return t.to(device=dev, dtype=torch.float32).contiguous()
+
+    re, im = dev_f32(adc_real), dev_f32(adc_imag)
+    tx, rx = dev_f32(tpos).reshape(-1, 3), dev_f32(rpos).reshape(-1, 3)
     A, S = re.shape
     if tx.shape[0] != A or rx.shape[0] != A:
         raise ValueError(f"antenna count mismatch: IF has {A} rows, positions {tx.shape[0]}/{rx.shape[0]}")

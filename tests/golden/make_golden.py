@@ -10,7 +10,7 @@ resampler's adjoint accumulates, so its gradient buffers start from a stored
 non-zero pattern.
 
     python tests/golden/make_golden.py --out tests/golden
-    python tests/golden/make_golden.py --only mf_3072ch_f32   # one case
+    python tests/golden/make_golden.py --only fullsize_mf3072ch_f32   # one case
 """
 from __future__ import annotations
 
@@ -204,7 +204,7 @@ def main(argv=None):
         print("wrote", name)
 
     if only is not None:
-        cases = {"mf_3072ch_f32": lambda: run_mf_3072ch(mf)}
+        cases = {"fullsize_mf3072ch_f32": lambda: run_mf_3072ch(mf)}
         unknown = only - set(cases)
         if unknown:
             raise SystemExit(f"--only supports {sorted(cases)}, not {sorted(unknown)}")
@@ -236,7 +236,7 @@ def main(argv=None):
     save("bilinear_f32", {**inp, **run_bilinear(st, inp)})
 
     # the reference's kernels at the full 3072-channel workload size
-    save("mf_3072ch_f32", run_mf_3072ch(mf))
+    save("fullsize_mf3072ch_f32", run_mf_3072ch(mf))
 
 
 if __name__ == "__main__":

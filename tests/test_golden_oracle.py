@@ -78,5 +78,22 @@ def test_bilinear_oracle_vs_reference(name):
 def test_golden_fixtures_present():
     names = golden_cases("")
     for expected in ("mf_scene_f32", "mf_odd_f32", "mf_scene_f16", "mf_scene_f64", "mf_fft_f32",
-                     "tracer_f32", "tracer_f64", "bilinear_f32"):
+                     "tracer_f32", "tracer_f64", "bilinear_f32", "fullsize_mf3072ch_f32"):
         assert expected in names
+
+
+def test_oracle_matches_reference_kernels_at_full_3072_channel_size():
+    """The oracle against the reference's own kernels run on the whole
+    3072-channel workload (3072 x 128 x 48^3; inputs regenerated from their seed):
+    the FP32 form within the reference's own FP32 phase error, the FP64 form too."""
+    from oracle import workload_parity as wp
+
+    g = load_golden("fullsize_mf3072ch_f32")
+    w = wp.mf3072_inputs(0)
+    sums = np.array([np.abs(w["re"].astype(np.float64)).sum(), np.abs(w["im"].astype(np.float64)).sum()])
+    np.testing.assert_allclose(sums, g["input_abs_sums"], rtol=1e-9)
+    vi = g["voxel_ids"]
+    ref = g["out_real"].astype(np.float64) + 1j * g["out_imag"]
+    yr, yi = orc.mf_forward(w["re"], w["im"], w["tx"], w["rx"], w["vox"][:, vi], w["fs"], w["As"], "f32")
+    assert rel_l2(yr + 1j * yi, ref) < REF_FP32_LEVEL
+    assert rel_l2(wp.mf_forward_ref(w, vi, "f64"), ref) < REF_FP32_LEVEL

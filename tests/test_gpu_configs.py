@@ -5,7 +5,7 @@ on subsets it finishes in seconds (oracle/workload_parity.py names them):
 * 3072 channels x 128 samples x 48^3 voxels: every voxel and antenna is run on
   the GPU; the forward is checked at 4096 voxels, the adjoint at 96 antenna
   rows.  The PLAIN form is also checked against the reference's own kernels at
-  this size (tests/golden/mf_3072ch_f32.npz).
+  this size (tests/golden/fullsize_mf3072ch_f32.npz).
 * 49152 channels x 256 samples x 128^3 voxels: the whole volume and the whole
   adjoint on the GPU; checked at a 16^3 voxel sub-lattice and 16 antenna rows.
 * The tracer on 64 antennas x 4096 rays x 128 samples of a random-init SDF
@@ -87,7 +87,7 @@ def test_mf3072_adjoint_vs_fp64(cuda, mf3072, parity_log):
 def test_mf3072_plain_matches_reference_kernels(cuda, mf3072, parity_log):
     """PLAIN forward and adjoint against the reference's own CUDA kernels run on
     the same full-size inputs (regenerated here from their seed)."""
-    gold = load_golden("mf_3072ch_f32")
+    gold = load_golden("fullsize_mf3072ch_f32")
     sums = np.array([np.abs(mf3072["re"].astype(np.float64)).sum(), np.abs(mf3072["im"].astype(np.float64)).sum()])
     np.testing.assert_allclose(sums, gold["input_abs_sums"], rtol=1e-9)
     vi, rows = gold["voxel_ids"], gold["rows"]

@@ -153,17 +153,19 @@ def test_bilinear_matches_reference_bitwise(cuda, name):
     np.testing.assert_array_equal(gs.cpu().numpy(), g["grad_sigmas"])
 
 
-@pytest.mark.parametrize("consistent", [False, True])
-def test_mf_fft_consistent_bins_flag(cuda, consistent):
-    """The range-bin kernels with the bound made consistent with the bin index
-    (an opt-in fix of MatchedFilter_cuda_kernel.cu:143-148) against the FP32
-    oracle with the same bound; the default stays the reference's."""
+ORACLE_FP32_LEVEL = 5e-4  # the FP32 oracle has no fused multiply-adds: the reference's FP32 phase level
+
+
+def _fft_flag_case(consistent):
+    """The range-bin kernels with and without the bound made consistent with the
+    bin index (an opt-in fix of MatchedFilter_cuda_kernel.cu:143-148) against the
+    FP32 oracle with the same bound; returns the adjoint's non-zero count."""
     from geraf_b200.ops.RFMatchedFilter import _C
 
     g = load_golden("mf_fft_f32")
     A, B = g["spec_real"].shape
     N = g["voxel"].shape[1]
-    spacing = 0.02
+    spacing = 0.0245  # the scene's delays (0.87-1.0 m) straddle the reference's bound 0.98 m
     args = [cu(g[k]) for k in ("spec_real", "spec_imag", "tx", "rx")]
     out_r = torch.full((N,), float("nan"), device="cuda")
     out_i = torch.full((N,), float("nan"), device="cuda")
@@ -179,8 +181,13 @@ def test_mf_fft_consistent_bins_flag(cuda, consistent):
     hr, hi = orc.mf_fft_backward(g["grad_output_real"], g["grad_output_imag"], g["tx"], g["rx"], g["voxel"], A,
                                  B, spacing, consistent)
     got = out_r.cpu().numpy() + 1j * out_i.cpu().numpy()
-    # the scene's delays (~0.95 m) lie between the two bounds (0.8 and 1.6 m)
-    assert (np.count_nonzero(got) > 0) == consistent
-    assert rel_l2(got, rr + 1j * ri) < 1e-5
-    assert rel_l2(h_r.cpu().numpy() + 1j * h_i.cpu().numpy(), hr + 1j * hi) < 1e-5
+    assert rel_l2(got, rr + 1j * ri) < ORACLE_FP32_LEVEL
+    assert rel_l2(h_r.cpu().numpy() + 1j * h_i.cpu().numpy(), hr + 1j * hi) < ORACLE_FP32_LEVEL
+    return np.count_nonzero(h_r.cpu().numpy())
+
+
+def test_mf_fft_consistent_bins_flag(cuda):
+    """The consistent bound keeps the delays between the reference's bound and
+    twice it; below it both agree with the oracle."""
+    assert _fft_flag_case(True) > _fft_flag_case(False) > 0
 

@@ -211,7 +211,7 @@ def test_launch_shapes_agree(cuda, fwd_tuning, bwd_tuning):
             gi = torch.randn(xr.shape, device="cuda", generator=g)
             keep = torch.isfinite(xr[:, 0])  # antenna 3 has no points: 0/0
             ((xr[keep] * gr[keep]).sum() + (xi[keep] * gi[keep]).sum()).backward()
-            outs.append([torch.complex(xr, xi)[keep].cpu().numpy()] +
+            outs.append([torch.complex(xr, xi)[keep].detach().cpu().numpy()] +
                         [t[k].grad.double().cpu().numpy() for k in ("sig", "nrm", "pts")])
         for a, b in zip(outs[0], outs[1]):
             assert rel_l2(b, a) < 2e-6

@@ -68,7 +68,10 @@ def test_sample_volume_kernel_matches_the_reference_host_sampling(cuda, mode, al
                                align).cpu().numpy()
     scale = np.abs(vol).max()
     assert np.max(np.abs(got - host)) < 1e-6 * scale
-    assert np.max(np.abs(got - orc.sample_volume(vol, pts, mode, align))) < 1e-6 * scale
+    # against exact arithmetic: the FP32 source index (up to ~40 here) is rounded to
+    # ~4e-6, which moves the interpolation weights by as much -- for torch as well
+    assert np.max(np.abs(got - orc.sample_volume(vol, pts, mode, align))) < 2e-5 * scale
+    assert np.max(np.abs(host - orc.sample_volume(vol, pts, mode, align))) < 2e-5 * scale
     assert np.all(got[40:44] == 0.0)
     nan_pts = torch.tensor([[np.nan, 0.0, 0.0], [0.0, 0.0, 0.0]], device="cuda")
     out = volume.sample_volume(torch.tensor(vol, device="cuda"), nan_pts, mode, align).cpu().numpy()
