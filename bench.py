@@ -177,28 +177,13 @@ def fp32_peak_tflops(dev) -> float:
     return best
 
 
-def horner_ceiling_tflops(dev) -> float:
-    """Measured rate of the MIXED forward's Horner loop alone (geraf_rf_horner_probe:
-    no per-(voxel, antenna) set-up), the ceiling of that loop's instruction form."""
-    import torch
-
+def loop_ceiling_tflops(dev) -> float:
+    """Measured rate of the MIXED forward's sample loop alone (geraf_rf_goertzel_probe:
+    the second-order recurrence on packed complex samples, 4 blocks per SM, no
+    per-(voxel, antenna) set-up), the ceiling of that loop's instruction form."""
     from benchkit import probes
 
-    lib = probes.lib()
-    sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    blocks, threads, rows = sms * 3, 128, 256
-    sink = torch.empty(blocks * threads, device=dev)
-    stream = torch.cuda.current_stream(dev).cuda_stream
-    best = 0.0
-    for _ in range(4):
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        probes.check(lib.geraf_rf_horner_probe(blocks, threads, rows, sink.data_ptr(), stream),
-                     "horner probe")
-        e.record()
-        e.synchronize()
-        best = max(best, blocks * threads * rows * 16384 / (s.elapsed_time(e) * 1e-3) / 1e12)
-    return best
+    return probes.measure("goertzel", 4, dev.index or 0)
 
 
 def make_mf_workload(name, rank, world, dev, seed):
@@ -394,7 +379,7 @@ def run_ours(args):
     e2e_value = world * triples / (e2e_ms * 1e-3) / 1e9
 
     peak = fp32_peak_tflops(dev)
-    ceiling = horner_ceiling_tflops(dev) if args.precision == "mixed" else None
+    ceiling = loop_ceiling_tflops(dev) if args.precision == "mixed" else None
     achieved = FLOPS_PER_TRIPLE * triples / (kms * 1e-3) / 1e12
     traffic = read_profile_traffic(args.workload)
     launches = launches_per_mf_call(wl, args.precision) * args.steps
@@ -428,12 +413,13 @@ def run_ours(args):
             "value": round(spec, 3), "unit": "TFLOP/s", "frac": round(achieved / spec, 4),
             "source": "SMs x 128 FP32 lanes x 2 flops x the median SM clock sampled in the timed region"}
     if ceiling is not None:
-        # The Horner loop alone, without the per-(voxel, antenna) set-up: the ceiling of
+        # The sample loop alone, without the per-(voxel, antenna) set-up: the ceiling of
         # the kernel's instruction form, below the FMA-rate peak (operand fetch).
         line["roofline"]["loop_ceiling"] = {
             "value": round(ceiling, 3), "unit": "TFLOP/s", "frac_of_peak": round(ceiling / peak, 4),
             "kernel_frac_of_ceiling": round(achieved / ceiling, 4),
-            "source": "geraf_rf_horner_probe (the forward's packed Horner loop alone) in this process"}
+            "source": "geraf_rf_goertzel_probe (the forward's second-order recurrence loop alone, "
+                      "4 blocks per SM) in this process"}
 
     # The extras are single-GPU measurements: under torchrun (N > 1) they would only hold
     # every GPU while rank 0 repeats them, so they run at N = 1 alone.
@@ -585,7 +571,7 @@ def _stage1_extra(args, dev) -> dict:
             st.capture()
         ms = autotune.time_call(st.run, iters=iters, warmup=1)
         res[name] = {"ms": round(ms, 2), "it_per_s": round(1e3 / ms, 2)}
-    eq = stage1_eval.compare(steps=args.stage1_steps, seed=args.seed, checkpoints=4)
+    eq = stage1_eval.compare(steps=args.stage1_steps, seed=args.seed, checkpoints=8)
     for form in ("mixed_graph", "plain_eager"):
         eq[form].pop("loss_every_10", None)
     return {"stage1_step": {"workload": ("128 antennas x 2048 rays x 128 target samples (64 coarse), S=256, "

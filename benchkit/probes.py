@@ -54,3 +54,43 @@ def lib():
 def check(status: int, what: str) -> None:
     if status != 0:
         raise RuntimeError(f"{what} failed with status {status}")
+
+
+def measure(name: str, blocks_per_sm: int, device=0) -> float:
+    """Best-of-5 rate of one probe in TFLOP/s (CUDA events on the current stream)."""
+    import torch
+
+    dev = torch.device("cuda", device)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    if name == "fma":
+        blocks, threads, arg, flops = sms * blocks_per_sm, 256, 1 << 12, 32
+    else:
+        blocks, threads, arg, flops = sms * blocks_per_sm, 128, 256, 16384
+    fn = getattr(lib(), f"geraf_rf_{name}_probe")
+    sink = torch.empty(blocks * threads, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        check(fn(blocks, threads, arg, sink.data_ptr(), stream), name)
+        e.record()
+        e.synchronize()
+        best = max(best, blocks * threads * arg * flops / (s.elapsed_time(e) * 1e-3) / 1e12)
+    return best
+
+
+def main() -> int:
+    """Prints the FP32 FMA rate and the two loop probes at 2-6 blocks per SM (JSON)."""
+    import json
+
+    res = {"fma_tflops": round(measure("fma", 8), 2)}
+    for bps in (2, 3, 4, 6):
+        for name in ("horner", "goertzel"):
+            res[f"{name}_{bps}_blocks_per_sm_tflops"] = round(measure(name, bps), 2)
+    print(json.dumps(res))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -146,8 +146,12 @@ def train(precision: str, graph: bool, steps: int, volume, half: float, power: f
     ref = torch.tensor(analytic_surface_points(20000, np.random.default_rng(seed + 7)), device=dev)
     curve = [(0, chamfer(sdf_surface_points(st.net, center, SDF_RADIUS), ref),
               sdf_on_surface(st.net, center, SDF_RADIUS, ref))]
+    # capture() runs two eager warm-up steps before it records one; the eager form
+    # takes the same two steps, so both forms start timing from the same state
     if graph:
         st.capture()
+    else:
+        st.warmup()
     st.gen.manual_seed(seed + 1)   # the same schedule of ray resamplings for both forms
     every = max(1, steps // checkpoints)
     losses = []

@@ -916,13 +916,12 @@ Tuning mf_forward_resolve(const MfArgs& a, const Tuning& req) {
   if (a.mode == kNufft) return mf_nufft_forward_resolve(a, req);
   Tuning t = req;
   if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = 128;
-  // MIXED runs voxel pairs through packed FMAs (2, 4 or 8 voxels per thread);
-  // eight amortise the shared-memory sample loads, loop control and the
-  // per-(voxel, antenna) phase set-up best (measured on B200: 128 threads x 8
-  // voxels x 8-antenna stages is the fastest shape for 49152 x 256 samples
-  // x 128^3 voxels).  PLAIN takes 1, 2 or 4.
+  // MIXED keeps 2, 4 or 8 voxels per thread, each with its own recurrence state;
+  // four measured fastest on B200 for 49152 x 256 samples x 128^3 voxels
+  // (50.0 TFLOP/s at 128 or 256 threads x 4 voxels, against 46.8 at 128 x 8:
+  // 124 against 242 registers, so twice the resident blocks).  PLAIN takes 1, 2 or 4.
   if (a.mode == kMixed) {
-    if (t.items != 2 && t.items != 4 && t.items != 8) t.items = t.items == 1 ? 2 : 8;
+    if (t.items != 2 && t.items != 4 && t.items != 8) t.items = t.items == 1 ? 2 : 4;
   } else if (t.items != 1 && t.items != 2 && t.items != 4) {
     t.items = 1;
   }

@@ -213,5 +213,6 @@ def test_launch_shapes_agree(cuda, fwd_tuning, bwd_tuning):
             ((xr[keep] * gr[keep]).sum() + (xi[keep] * gi[keep]).sum()).backward()
             outs.append([torch.complex(xr, xi)[keep].detach().cpu().numpy()] +
                         [t[k].grad.double().cpu().numpy() for k in ("sig", "nrm", "pts")])
+        # work items of other sizes group the per-antenna partial sums differently
         for a, b in zip(outs[0], outs[1]):
-            assert rel_l2(b, a) < 2e-6
+            assert rel_l2(b, a) < 5e-6
