@@ -135,6 +135,7 @@ __global__ void __launch_bounds__(kSpreadThreads) nufft_tracer_spread_kernel(con
     const float nrm[3] = {cur.nx, cur.ny, cur.nz};
     const float pt[3] = {cur.px, cur.py, cur.pz};
     const float sig = cur.sig;
+    if (surely_culled(txp, rxp, nrm, pt)) continue;
     SpecGeom geo;
     specular_geometry(txp, rxp, nrm, pt, geo);
     if (culled(geo)) continue;
@@ -304,7 +305,7 @@ __global__ void __launch_bounds__(128) nufft_tracer_gather_kernel(const TrGather
       const float rxp[3] = {static_cast<float>(ps[3]), static_cast<float>(ps[4]), static_cast<float>(ps[5])};
       SpecGeom geo;
       bool live = false;
-      if (active) {
+      if (active && !surely_culled(txp, rxp, nrm, pt)) {
         specular_geometry(txp, rxp, nrm, pt, geo);
         live = !culled(geo);
       }

@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(256) ragged_fwd_kernel(const RgP<T> p) {
     for (int64_t p0 = pt_begin; p0 < pt_end; p0 += TILE) {
       bool valid = false;
       float2 w = make_float2(0.0f, 0.0f), zt = make_float2(1.0f, 0.0f), zk = make_float2(1.0f, 0.0f);
-      if (inb) {
+      if (inb && !surely_culled(txp, rxp, nrm, pt)) {
         SpecGeom geo;
         specular_geometry(txp, rxp, nrm, pt, geo);
         if (!culled(geo)) {
@@ -399,9 +399,11 @@ __global__ void __launch_bounds__(kBwdThreads) ragged_bwd_kernel(const RgP<T> p,
         ld3(p.points, pi, pt);
         ld3(p.tx, a, txp);
         ld3(p.rx, a, rxp);
-        SpecGeom geo;
-        specular_geometry(txp, rxp, nrm, pt, geo);
-        live = !culled(geo);
+        if (!surely_culled(txp, rxp, nrm, pt)) {
+          SpecGeom geo;
+          specular_geometry(txp, rxp, nrm, pt, geo);
+          live = !culled(geo);
+        }
       }
       if (!live) {
         p.g_sigmas[pi] = from_f<T>(0.0f);

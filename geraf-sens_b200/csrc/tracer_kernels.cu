@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(256) tracer_fwd_mixed_kernel(const TrP<T> p) {
   for (int64_t p0 = pt_begin; p0 < pt_end; p0 += TILE) {
     bool valid = false;
     float2 w = make_float2(0.0f, 0.0f), zt = make_float2(1.0f, 0.0f), zk = make_float2(1.0f, 0.0f);
-    if (inb) {
+    if (inb && !surely_culled(txp, rxp, nrm, pt)) {
       SpecGeom geo;
       specular_geometry(txp, rxp, nrm, pt, geo);
       if (!culled(geo)) {
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(128, 6) tracer_bwd_mixed_kernel(const TrP<T> p
       const float txp[3] = {ps[0], ps[1], ps[2]};
       const float rxp[3] = {ps[3], ps[4], ps[5]};
       bool live = false;
-      if (active) {
+      if (active && !surely_culled(txp, rxp, own_nrm, own_pt)) {
         SpecGeom geo;
         specular_geometry(txp, rxp, own_nrm, own_pt, geo);
         live = !culled(geo);

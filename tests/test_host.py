@@ -217,3 +217,66 @@ def test_missing_library_fails_loudly():
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
     assert out.returncode == 0, out.stderr[-2000:]
     assert "raised:" in out.stdout and "not found" in out.stdout
+
+
+def _surely_culled_f32(tx, rx, n, p):
+    """numpy FP32 restatement of surely_culled() in csrc/tracer_geometry.cuh."""
+    f = np.float32
+    i = (p - tx).astype(f)
+    o = (rx - p).astype(f)
+    inn = (i * n).sum(-1, dtype=f)
+    ii, nn = (i * i).sum(-1, dtype=f), (n * n).sum(-1, dtype=f)
+    back = (inn > 0) & (inn * inn > f(1e-8) * (ii * nn))
+    r = (i - f(2.0) * inn[:, None] * n).astype(f)
+    orr = (o * r).sum(-1, dtype=f)
+    m = f(1.0) + f(2.0) * nn
+    away = (orr < 0) & (orr * orr > f(1e-8) * ((o * o).sum(-1, dtype=f) * ii * (m * m)))
+    return back | away
+
+
+def _culled_reference_f32(tx, rx, n, p):
+    """The reference's FP32 culling (SignalTracer_cuda_kernel.cu:172-197, 417-420)."""
+    f = np.float32
+
+    def normalize(v):
+        return (v * (f(1.0) / (np.sqrt((v * v).sum(-1, dtype=f)) + f(1e-7)))[:, None]).astype(f)
+
+    inc = normalize((p - tx).astype(f))
+    idn = (inc * n).sum(-1, dtype=f)
+    refl = normalize((inc - f(2.0) * idn[:, None] * n).astype(f))
+    ret = normalize((rx - p).astype(f))
+    align = (ret * refl).sum(-1, dtype=f)
+    return (align < f(1e-6)) | (idn > 0)
+
+
+def test_early_cull_is_conservative():
+    """Every pair the tracer kernels' early test culls is culled by the reference's
+    FP32 geometry, on random and near-boundary pairs with unit and non-unit normals
+    (the early test only skips work the exact form would discard)."""
+    rng = np.random.default_rng(0)
+    f = np.float32
+    total = kept_early = 0
+    for trial in range(8):
+        M = 400_000
+        tx = rng.normal(0, 0.05, (M, 3)).astype(f)
+        rx = (tx + rng.normal(0, 0.01, (M, 3))).astype(f)
+        p = (np.array([0, 0, 0.4]) + rng.normal(0, 0.1, (M, 3))).astype(f)
+        n = rng.normal(0, 1, (M, 3))
+        n /= np.linalg.norm(n, axis=1, keepdims=True)
+        if trial % 2:   # non-unit normals
+            n *= rng.uniform(0.1, 3.0, (M, 1))
+        i = (p - tx).astype(np.float64)
+        if trial in (4, 5):  # push pairs onto the back-facing boundary, i.n = 0
+            n -= ((i * n).sum(1) / (i * i).sum(1))[:, None] * i * rng.uniform(0.999, 1.001, (M, 1))
+        if trial in (6, 7):  # and onto the alignment boundary, o.r = 0
+            r = i - 2.0 * (i * n).sum(1)[:, None] * n / (n * n).sum(1)[:, None]
+            o = rng.normal(0, 1, (M, 3))
+            o -= ((o * r).sum(1) / (r * r).sum(1))[:, None] * r * rng.uniform(0.999, 1.001, (M, 1))
+            rx = (p + 0.3 * o / np.linalg.norm(o, axis=1, keepdims=True)).astype(f)
+        n = n.astype(f)
+        early = _surely_culled_f32(tx, rx, n, p)
+        exact = _culled_reference_f32(tx, rx, n, p)
+        assert not np.any(early & ~exact)
+        total += M
+        kept_early += int(early.sum())
+    assert kept_early > total // 4  # the early test does take most culled pairs
