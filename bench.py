@@ -737,6 +737,33 @@ def tracer_live_pairs(tw, chunk: int = 8) -> int:
     return live
 
 
+def tracer_listed_points(tw) -> int:
+    """Points that the MIXED tracer's per-point pre-cull keeps (the in-bounds
+    points it cannot cull for every antenna; csrc/tracer_precull.cu), restated in
+    torch FP64 on the device."""
+    import torch
+
+    d = torch.float64
+    tx, rx = tw["tx"].to(d), tw["rx"].to(d)
+    ct, cr = tx.mean(0), rx.mean(0)
+    rt = (tx - ct).norm(dim=1).max()
+    rr = (rx - cr).norm(dim=1).max()
+    rt = rt + 1e-12 * (rt + ct.abs().sum())
+    rr = rr + 1e-12 * (rr + cr.abs().sum())
+    n, p = tw["normals"].to(d), tw["points"].to(d)
+    ic, oc = p - ct, cr - p
+    nn = (n * n).sum(1)
+    nrm, m = nn.sqrt(), 1.0 + 2.0 * nn
+    icn = (ic * n).sum(1)
+    ni, no = ic.norm(dim=1), oc.norm(dim=1)
+    back = icn - rt * nrm > 1e-4 * (ni + rt) * nrm
+    hi = ic - 2.0 * icn[:, None] * n
+    ho = oc - 2.0 * (oc * n).sum(1)[:, None] * n
+    bound = (oc * hi).sum(1) + rr * hi.norm(dim=1) + rt * ho.norm(dim=1) + m * rr * rt
+    away = bound < -1e-4 * (no + rr) * (ni + rt) * m
+    return int((tw["inbounds"] & ~(back | away)).sum())
+
+
 def _tracer_extra(args, dev, art) -> dict:
     """Tracer forward + adjoint (with position gradients) on the 64-antenna x
     4096-ray x 128-sample workload of a random-init SDF network: MIXED (launch
@@ -807,6 +834,7 @@ def _tracer_extra(args, dev, art) -> dict:
     flops_live = 12.0 * live * St
     ms_m = tr["mixed"]["ms"]
     roof = {"flops_per_triple": 12, "live_pair_fraction": round(live / (At * P), 4),
+            "listed_point_fraction": round(tracer_listed_points(tw) / P, 4),
             "achieved_all_tflops": round(flops_all / (ms_m * 1e-3) / 1e12, 3),
             "achieved_live_tflops": round(flops_live / (ms_m * 1e-3) / 1e12, 3)}
     if peak:
@@ -814,7 +842,9 @@ def _tracer_extra(args, dev, art) -> dict:
         roof["frac_all"] = round(flops_all / (ms_m * 1e-3) / 1e12 / peak, 4)
         roof["frac_live"] = round(flops_live / (ms_m * 1e-3) / 1e12 / peak, 4)
         roof["note"] = ("frac_live is the roofline: culled pairs carry no samples to sum; frac_all "
-                        "counts every triple as the reference's kernels visit them")
+                        "counts every triple as the reference's kernels visit them.  The kernels form "
+                        "the geometry of every pair of the points the per-point pre-cull keeps "
+                        "(listed_point_fraction) and sum the samples of live pairs only")
     res["tracer"] = {"workload": f"{At} antennas x {tw['rays']} rays x {P // tw['rays']} samples, S={St}",
                      "unit": "rays/s (ray = ray x antenna pair)", "mixed_with_point_grads": tr["mixed"],
                      "nufft_with_point_grads": tr["nufft"], "plain": tr["plain"], "roofline": roof,

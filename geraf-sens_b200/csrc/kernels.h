@@ -128,6 +128,20 @@ Tuning tracer_backward_resolve(const TracerArgs& a, const Tuning& req);
 size_t tracer_backward_workspace(const TracerArgs& a, const Tuning& t);
 cudaError_t tracer_backward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st);
 
+// Point pre-cull of the MIXED tracer (tracer_precull.cu): the in-bounds points
+// that a conservative per-point test cannot cull for every antenna of the call,
+// listed in ascending order in a workspace region of tracer_point_list_bytes(P)
+// bytes, with their count on the device.  With zero_grads the adjoint's
+// gradients of every point left out are written as zeros.
+struct PointList {
+  const int* list;
+  const int* count;
+};
+bool tracer_point_list_applies(const TracerArgs& a);
+size_t tracer_point_list_bytes(int64_t P);
+PointList tracer_point_list_view(void* ws, int64_t P);
+cudaError_t tracer_point_list(const TracerArgs& a, void* ws, bool zero_grads, cudaStream_t st);
+
 // Fast approximate tracer (MODE_NUFFT, nufft_tracer_kernels.cu); the generic
 // tracer_* entry points dispatch here for that mode.
 Tuning tracer_nufft_forward_resolve(const TracerArgs& a, const Tuning& req);

@@ -280,3 +280,75 @@ def test_early_cull_is_conservative():
         total += M
         kept_early += int(early.sum())
     assert kept_early > total // 4  # the early test does take most culled pairs
+
+
+def _aperture_f64(tx, rx):
+    """numpy restatement of aperture_kernel() in csrc/tracer_precull.cu."""
+    t, r = tx.astype(np.float64), rx.astype(np.float64)
+    ct, cr = t.mean(0), r.mean(0)
+    rt = np.sqrt(((t - ct) ** 2).sum(1)).max()
+    rr = np.sqrt(((r - cr) ** 2).sum(1)).max()
+    rt += 1e-12 * (rt + np.abs(ct).sum())
+    rr += 1e-12 * (rr + np.abs(cr).sum())
+    return ct, rt, cr, rr
+
+
+def _culled_for_all_f64(ap, n, p):
+    """numpy restatement of culled_for_all() in csrc/tracer_precull.cu."""
+    ct, rt, cr, rr = ap
+    n = n.astype(np.float64)
+    ic = p.astype(np.float64) - ct
+    oc = cr - p.astype(np.float64)
+    nn = (n * n).sum(1)
+    nrm = np.sqrt(nn)
+    m = 1.0 + 2.0 * nn
+    icn = (ic * n).sum(1)
+    ni = np.sqrt((ic * ic).sum(1))
+    no = np.sqrt((oc * oc).sum(1))
+    back = icn - rt * nrm > 1e-4 * (ni + rt) * nrm
+    hi = ic - 2.0 * icn[:, None] * n
+    ho = oc - 2.0 * (oc * n).sum(1)[:, None] * n
+    bound = (oc * hi).sum(1) + rr * np.sqrt((hi * hi).sum(1)) + rt * np.sqrt((ho * ho).sum(1)) + m * rr * rt
+    away = bound < -1e-4 * (no + rr) * (ni + rt) * m
+    return back | away
+
+
+def test_point_precull_is_conservative():
+    """Every point the tracer's per-point pre-cull leaves out is culled for every
+    antenna of the call by the reference's FP32 geometry: compact and wide
+    apertures, unit and non-unit normals, and points pushed onto the boundary of
+    the back-facing bound (the pre-cull only skips work the exact form discards)."""
+    rng = np.random.default_rng(1)
+    f = np.float32
+    skipped = total = 0
+    for trial in range(8):
+        A, M = 48, 60_000
+        spread = (0.002, 0.02, 0.1, 0.3)[trial % 4]
+        tx = (np.array([0.0, 0.0, 0.0]) + rng.normal(0, spread, (A, 3))).astype(f)
+        rx = (tx + rng.normal(0, spread / 2, (A, 3))).astype(f)
+        p = (np.array([0, 0, 0.4]) + rng.normal(0, 0.15, (M, 3))).astype(f)
+        n = rng.normal(0, 1, (M, 3))
+        n /= np.linalg.norm(n, axis=1, keepdims=True)
+        if trial >= 4:
+            n *= rng.uniform(0.1, 3.0, (M, 1))
+        ap = _aperture_f64(tx, rx)
+        if trial in (2, 6):
+            # normals tilted so that i_c.n - R_t|n| sits just above the margin
+            ct, rt = ap[0], ap[1]
+            ic = p.astype(np.float64) - ct
+            d = np.linalg.norm(ic, axis=1)
+            u = ic / d[:, None]
+            cos_a = np.minimum((rt + 1e-4 * (d + rt)) / d * (1 + rng.uniform(1e-9, 1e-6, M)), 1.0)
+            w = rng.normal(0, 1, (M, 3))
+            w -= (w * u).sum(1)[:, None] * u
+            w /= np.linalg.norm(w, axis=1, keepdims=True)
+            scale = np.linalg.norm(n, axis=1)[:, None]
+            n = (cos_a[:, None] * u + np.sqrt(1 - cos_a ** 2)[:, None] * w) * scale
+        n = n.astype(f)
+        skip = _culled_for_all_f64(ap, n, p)
+        for a in range(A):
+            exact = _culled_reference_f32(np.broadcast_to(tx[a], p.shape), np.broadcast_to(rx[a], p.shape), n, p)
+            assert not np.any(skip & ~exact), (trial, a)
+        skipped += int(skip.sum())
+        total += M
+    assert skipped > total // 4  # most points facing away are left out
