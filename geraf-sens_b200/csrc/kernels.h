@@ -128,7 +128,7 @@ Tuning tracer_backward_resolve(const TracerArgs& a, const Tuning& req);
 size_t tracer_backward_workspace(const TracerArgs& a, const Tuning& t);
 cudaError_t tracer_backward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st);
 
-// Point pre-cull of the MIXED tracer (tracer_precull.cu): the in-bounds points
+// Point pre-cull of the MIXED and NUFFT tracers (tracer_precull.cu): the in-bounds points
 // that a conservative per-point test cannot cull for every antenna of the call,
 // listed in ascending order in a workspace region of tracer_point_list_bytes(P)
 // bytes, with their count on the device.  With zero_grads the adjoint's
@@ -152,9 +152,11 @@ size_t tracer_nufft_backward_workspace(const TracerArgs& a, const Tuning& t);
 cudaError_t tracer_nufft_backward(const TracerArgs& a, const Tuning& t, void* ws, cudaStream_t st);
 
 // Sums `splits` [P][6] partial point gradients in split order and divides by P
-// into grad_normals (and grad_points when non-null).
+// into grad_normals (and grad_points when non-null); with a point list, only
+// the listed points'.
 cudaError_t launch_tracer_bwd_finalize(int dtype, const float* partial, int splits, int64_t P, void* g_normals,
-                                       void* g_points, cudaStream_t st);
+                                       void* g_points, cudaStream_t st, const int* plist = nullptr,
+                                       const int* plist_count = nullptr);
 
 // Batched tracer over antennas with uneven point sets (CSR point_offsets [A+1]).
 struct RaggedArgs {

@@ -46,6 +46,10 @@ struct TrSpreadP {
   const float* bbox;  // [6]
   float2* grid;       // [vsplits][A][M]
   int* status;
+  // the points left by the per-point pre-cull and their number (device);
+  // null: every in-bounds point is visited
+  const int* plist;
+  const int* plist_count;
   int64_t A, P, pts_per_split;
   int M, h, vsplits;
   double k0, b0, k1, b1;
@@ -56,11 +60,14 @@ struct SpreadPoint {
   bool inb;
 };
 
+// Loads the point at position k: listed point list[k], or point k.
 template <typename T>
-__device__ __forceinline__ SpreadPoint load_spread_point(const TrSpreadP<T>& p, int64_t a, int64_t q,
+__device__ __forceinline__ SpreadPoint load_spread_point(const TrSpreadP<T>& p, int64_t a, int64_t k,
                                                          int64_t p_end) {
   SpreadPoint s{0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, false};
-  s.inb = q < p_end && p.inb[q];
+  if (k >= p_end) return s;
+  const int64_t q = p.plist != nullptr ? static_cast<int64_t>(p.plist[k]) : k;
+  s.inb = p.plist != nullptr || p.inb[q];  // listed points are in bounds
   if (s.inb) {
     s.nx = ld_f(p.normals, q * 3 + 0);
     s.ny = ld_f(p.normals, q * 3 + 1);
@@ -121,8 +128,10 @@ __global__ void __launch_bounds__(kSpreadThreads) nufft_tracer_spread_kernel(con
 
   const float txp[3] = {static_cast<float>(pos[0]), static_cast<float>(pos[1]), static_cast<float>(pos[2])};
   const float rxp[3] = {static_cast<float>(pos[3]), static_cast<float>(pos[4]), static_cast<float>(pos[5])};
-  const int64_t p_begin = static_cast<int64_t>(vs) * p.pts_per_split;
-  const int64_t p_end = min(p.P, p_begin + p.pts_per_split);
+  const int64_t npts = p.plist != nullptr ? static_cast<int64_t>(*p.plist_count) : p.P;
+  const int64_t per_split = p.plist != nullptr ? (npts + p.vsplits - 1) / p.vsplits : p.pts_per_split;
+  const int64_t p_begin = static_cast<int64_t>(vs) * per_split;
+  const int64_t p_end = min(npts, p_begin + per_split);
   float* col_re = buf + threadIdx.x;
   float* col_im = buf + kWin * kWinLd + threadIdx.x;
   // The next point's inputs are loaded while the current one is spread (the
@@ -236,6 +245,8 @@ struct TrGatherP {
   T* g_points;
   float* partial;  // [splits][P][6] when splits > 1
   int* status;
+  const int* plist;  // as in TrSpreadP
+  const int* plist_count;
   int64_t A, P, per_split;
   int M, h, rows, splits;
   double k0, b0, k1, b1;
@@ -253,12 +264,18 @@ __global__ void __launch_bounds__(128) nufft_tracer_gather_kernel(const TrGather
 
   const int split = blockIdx.x % p.splits;
   const int64_t ptile = blockIdx.x / p.splits;
-  const int64_t pi = ptile * blockDim.x + threadIdx.x;
+  // thread t owns point position k (listed point list[k], or point k); the grid
+  // covers all P points and blocks past the listed ones have nothing to do
+  const int64_t npts = p.plist != nullptr ? static_cast<int64_t>(*p.plist_count) : p.P;
+  const int64_t p_base = ptile * blockDim.x;
+  if (p_base >= npts) return;
+  const int64_t k_own = p_base + threadIdx.x;
+  const bool inside = k_own < npts;
+  const int64_t pi = !inside ? 0 : p.plist != nullptr ? static_cast<int64_t>(p.plist[k_own]) : k_own;
   const int64_t a_begin = static_cast<int64_t>(split) * p.per_split;
   const int64_t a_end = min(p.A, a_begin + p.per_split);
   const int ntiles = a_end > a_begin ? ceil_div(a_end - a_begin, p.rows) : 0;
-  const bool inside = pi < p.P;
-  const bool active = inside && p.inb[pi];
+  const bool active = inside && (p.plist != nullptr || p.inb[pi]);
   const int mask = p.M - 1;
   const float fM = static_cast<float>(p.M);
 
@@ -411,7 +428,7 @@ struct TrNufftShape {
   // adjoint
   int rows = 4, splits = 1;
   int64_t ant_per_split = 0;
-  size_t deconv_off = 0, bbox_off = 0, grid_off = 0, grid2_off = 0, partial_off = 0, total = 0;
+  size_t deconv_off = 0, bbox_off = 0, grid_off = 0, grid2_off = 0, partial_off = 0, list_off = 0, total = 0;
   size_t pos_off = 128, buf_off = 0, smem = 0;
 };
 
@@ -449,6 +466,8 @@ TrNufftShape tr_shape(const TracerArgs& a, const Tuning& t, bool backward) {
     s.total = s.partial_off + (s.splits > 1 ? align256(static_cast<size_t>(s.splits) * a.P * 6 * sizeof(float)) : 0);
     s.smem = gather_smem_tr(s.rows, s.Mp, &s.buf_off);
   }
+  s.list_off = s.total;
+  if (tracer_point_list_applies(a)) s.total = s.list_off + tracer_point_list_bytes(a.P);
   return s;
 }
 
@@ -488,6 +507,15 @@ cudaError_t launch_tracer_nufft_forward(const TracerArgs& a, const Tuning& t, vo
   sp.bbox = bbox;
   sp.grid = grid;
   sp.status = device_status_ptr();
+  sp.plist = nullptr;
+  sp.plist_count = nullptr;
+  if (tracer_point_list_applies(a)) {
+    err = tracer_point_list(a, base + s.list_off, false, st);
+    if (err != cudaSuccess) return err;
+    const PointList pl = tracer_point_list_view(base + s.list_off, a.P);
+    sp.plist = pl.list;
+    sp.plist_count = pl.count;
+  }
   sp.A = a.A;
   sp.P = a.P;
   sp.pts_per_split = s.pts_per_split;
@@ -586,6 +614,16 @@ cudaError_t launch_tracer_nufft_backward(const TracerArgs& a, const Tuning& t, v
   p.g_points = static_cast<T*>(a.grad_points);
   p.partial = reinterpret_cast<float*>(base + s.partial_off);
   p.status = device_status_ptr();
+  p.plist = nullptr;
+  p.plist_count = nullptr;
+  if (tracer_point_list_applies(a)) {
+    // lists the points and zeroes the gradients of every point it leaves out
+    err = tracer_point_list(a, base + s.list_off, true, st);
+    if (err != cudaSuccess) return err;
+    const PointList pl = tracer_point_list_view(base + s.list_off, a.P);
+    p.plist = pl.list;
+    p.plist_count = pl.count;
+  }
   p.A = a.A;
   p.P = a.P;
   p.per_split = s.ant_per_split;
@@ -614,7 +652,7 @@ cudaError_t launch_tracer_nufft_backward(const TracerArgs& a, const Tuning& t, v
   if (err != cudaSuccess) return err;
   if (s.splits > 1) {
     err = launch_tracer_bwd_finalize(a.dtype, p.partial, s.splits, a.P, a.grad_normals,
-                                     with_points ? a.grad_points : nullptr, st);
+                                     with_points ? a.grad_points : nullptr, st, p.plist, p.plist_count);
   }
   return err;
 }
@@ -669,7 +707,9 @@ Tuning tracer_nufft_backward_resolve(const TracerArgs& a, const Tuning& req) {
   }
   const int64_t rows_total = std::max<int64_t>(1, (a.A + t.stage_rows - 1) / t.stage_rows);
   if (t.splits <= 0) {
-    const int64_t ptiles = std::max<int64_t>(1, (a.P + t.threads - 1) / t.threads);
+    int64_t ptiles = std::max<int64_t>(1, (a.P + t.threads - 1) / t.threads);
+    // only the blocks of points the pre-cull lists have work; a quarter is assumed
+    if (tracer_point_list_applies(a)) ptiles = std::max<int64_t>(1, ptiles / 4);
     const int per_sm = std::max(1, 1024 / t.threads);
     t.splits = pick_splits(ptiles, per_sm, dev.sm_count, rows_total);
   }

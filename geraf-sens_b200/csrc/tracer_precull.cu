@@ -313,7 +313,7 @@ cudaError_t launch_point_list(const TracerArgs& a, void* ws, bool zero_grads, cu
 
 bool tracer_point_list_applies(const TracerArgs& a) {
   // int32 indices and a grid of one block per 1024-point chunk
-  return a.mode == kMixed && a.P > 0 && a.P <= (int64_t{1} << 31) - kChunk;
+  return (a.mode == kMixed || a.mode == kNufft) && a.P > 0 && a.P <= (int64_t{1} << 31) - kChunk;
 }
 
 size_t tracer_point_list_bytes(int64_t P) { return list_layout(P).bytes; }

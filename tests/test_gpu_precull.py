@@ -134,3 +134,29 @@ def test_precull_out_of_bounds_and_non_finite(scene):
     nrm[2] = np.nan  # in bounds
     x = _c(tracer_forward(w, w["S"], "mixed"))
     assert np.isnan(x).all()
+
+
+def test_precull_nufft_form(scene):
+    """The NUFFT tracer reads the same point list: live pairs keep their sigma
+    gradient, culled pairs and points left out get exact zeros, the results agree
+    with the MIXED form to the NUFFT's accuracy, and an empty list gives zeros."""
+    w, live, dead = scene
+    A = w["sigmas"].shape[0]
+    g = wp.residual(A, w["S"], 7)
+    gn, gs, gp = tracer_backward(w, g.real.copy(), g.imag.copy(), "nufft", tuning={"splits": 2})
+    assert np.isfinite(gs).all() and np.isfinite(gn).all() and np.isfinite(gp).all()
+    assert (gs[live] != 0).all() and (gs[dead] == 0).all()
+    none_live = dead.all(0)
+    assert (gn[none_live] == 0).all() and (gp[none_live] == 0).all()
+    mn, ms, mp = tracer_backward(w, g.real.copy(), g.imag.copy(), "mixed")
+    assert wp.rel(gs, ms) < 1e-4 and wp.rel(gn, mn) < 1e-4 and wp.rel(gp, mp) < 1e-4
+    x = _c(tracer_forward(w, w["S"], "nufft"))
+    assert wp.rel(x, _c(tracer_forward(w, w["S"], "mixed"))) < 1e-4
+
+    w = dict(w)
+    away = w["points"].astype(np.float64) - w["tx"].astype(np.float64).mean(0)
+    w["normals"] = (away / np.linalg.norm(away, axis=1, keepdims=True)).astype(np.float32)
+    xr, xi = tracer_forward(w, w["S"], "nufft")
+    assert (xr == 0).all() and (xi == 0).all()
+    gn, gs, gp = tracer_backward(w, g.real.copy(), g.imag.copy(), "nufft")
+    assert (gn == 0).all() and (gs == 0).all() and (gp == 0).all()
