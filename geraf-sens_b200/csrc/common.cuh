@@ -238,6 +238,20 @@ __device__ __forceinline__ float2 cis_cycles(float x) {
   return make_float2(c, s);
 }
 
+// e^{j 2 pi x} for |x| <= 1/2 from the hardware sine and cosine (__sincosf,
+// absolute error ~4e-7 on [-pi, pi]): for the phasor that multiplies a term
+// once (its carrier or start phase), and for a rotator raised to at most
+// kFastPowers powers (per 64-sample block, per sample group), whose phase error
+// then stays below ~3e-6 rad, far inside the MIXED form's bound.  The
+// per-sample rotators, and block or group rotators of longer rows, keep
+// cis_cycles: their error grows with the steps they take.
+constexpr int kFastPowers = 8;
+__device__ __forceinline__ float2 cis_cycles_fast(float x) {
+  float s, c;
+  __sincosf(6.28318530717958647692f * x, &s, &c);
+  return make_float2(c, s);
+}
+
 // cosf(x) and sinf(x) from one sincosf call.  sincosf returns the same bits as
 // the two separate calls for every FP32 input -- geraf_rf_sincos_identity_check
 // compares all 2^32 inputs on the device -- so the PLAIN kernels keep the

@@ -159,6 +159,9 @@ __global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
     }
     __syncthreads();
     constexpr int B = 64;  // samples per Goertzel block
+    // z^B is raised to at most nb - 1 powers; up to 8 blocks its hardware phasor
+    // is accurate enough (phase error <= 8 x 4e-7 rad)
+    const bool few_blocks = (p.ld + B - 1) / B <= kFastPowers;
     for (int r = 0; r < rws; ++r) {
       const double* ps = pos + (s * p.rows + r) * 6;
       const double tx = ps[0], ty = ps[1], tz = ps[2], rx = ps[3], ry = ps[4], rz = ps[5];
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
         C2[j] = make_float2(2.0f * c1.x, 2.0f * c1.x);
         sn[j] = c1.y;
         const float kb = pc.dcyc * static_cast<float>(B);
-        const float2 zb = cis_cycles(kb - rintf(kb));
+        const float2 zb = few_blocks ? cis_cycles_fast(kb - rintf(kb)) : cis_cycles(kb - rintf(kb));
         ZB[j] = make_float2(zb.x, -zb.y);  // z^B
         R[j] = make_float2(0.0f, 0.0f);
       }
@@ -216,7 +219,7 @@ __global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
       }
 #pragma unroll
       for (int j = 0; j < VPT; ++j) {
-        const float2 c0 = cis_cycles(frac0[j]);
+        const float2 c0 = cis_cycles_fast(frac0[j]);
         const float2 e0 = make_float2(c0.x, -c0.y);  // exp(-j phi0)
         const float2 term = cmul(e0, R[j]);
         kahan_add(yr[j], cr[j], term.x);
@@ -432,12 +435,12 @@ __global__ void __launch_bounds__(256) mf_bwd_mixed_kernel(const MfBwdP<T> p) {
           const double c = static_cast<double>(pc.frac0) + static_cast<double>(n_begin) * pc.dcyc;
           start = static_cast<float>(c - rint(c));
         }
-        const float2 e = cis_cycles(start);
+        const float2 e = cis_cycles_fast(start);
         const float2 gv = make_float2(ld_f(p.gr, v), ld_f(p.gi, v));
         w = cmul(gv, e);
         zt = cis_cycles(pc.dcyc);
         const float kc = pc.dcyc * static_cast<float>(K);
-        zk = cis_cycles(kc - rintf(kc));
+        zk = G <= kFastPowers ? cis_cycles_fast(kc - rintf(kc)) : cis_cycles(kc - rintf(kc));
       }
       zeta[threadIdx.x] = zt;
       for (int gg = 0; gg < G; ++gg) {

@@ -203,11 +203,11 @@ __global__ void __launch_bounds__(256) tracer_fwd_mixed_kernel(const TrP<T> p) {
           const double c = static_cast<double>(pc.frac0) + static_cast<double>(n_begin) * pc.dcyc;
           start = static_cast<float>(c - rint(c));
         }
-        const float2 e = cis_cycles(start);
+        const float2 e = cis_cycles_fast(start);
         w = make_float2(amp * e.x, amp * e.y);
         zt = cis_cycles(pc.dcyc);
         const float kc = pc.dcyc * static_cast<float>(K);
-        zk = cis_cycles(kc - rintf(kc));
+        zk = G <= kFastPowers ? cis_cycles_fast(kc - rintf(kc)) : cis_cycles(kc - rintf(kc));
         valid = true;
       }
     }
@@ -652,7 +652,7 @@ __global__ void __launch_bounds__(128, 6) tracer_bwd_mixed_kernel(const TrP<T> p
       const float2 qc = cmul(zc, make_float2(pr.y, pim.y));
       const float qr = pr.x + qc.x;
       const float qi = -(pim.x + qc.y);
-      const float2 e0 = cis_cycles(pc.frac0);
+      const float2 e0 = cis_cycles_fast(pc.frac0);
       const float2 eq = cmul(e0, make_float2(qr, qi));
       // sum_n (g_r cos + g_i sin) = Re(exp(j phi0) Q)
       const float sum_re = eq.x;

@@ -20,10 +20,12 @@
 // 1e-4 margin.  Non-finite values fail both comparisons, so such points are
 // listed and decided by the exact form.  Out-of-bounds points are never listed.
 //
-// Four launches: the aperture bounds (one block), per-point flags with a count
-// per 1024-point chunk, an exclusive scan of the counts (one block), and the
-// ordered scatter of the listed point indices, which for the adjoint also
-// writes the zero gradients of every point not listed.
+// Launches: per-point flags with a count per 1024-point chunk, and the ordered
+// scatter of the listed point indices, which for the adjoint also writes the
+// zero gradients of every point not listed.  Each flags block bounds the
+// aperture itself and each scatter block sums the counts before its chunk,
+// up to 2048 antennas and 2048 chunks; beyond those, one-block kernels bound
+// the aperture and scan the counts once.
 #include <algorithm>
 #include <cmath>
 
@@ -34,20 +36,27 @@ namespace geraf {
 namespace {
 
 constexpr int kChunk = 1024;        // points per flag chunk (32 words)
-constexpr int kChunkThreads = 256;  // 4 points per thread
+constexpr int kChunkThreads = 256;  // 4 points per thread (faster than 1024 x 1)
+// Up to these sizes the flags kernel bounds the aperture in every block and the
+// scatter kernel sums the preceding chunks' counts itself: two launches, not four.
+constexpr int64_t kInlineApertureMax = 2048;  // antennas
+constexpr int64_t kInlineScanMax = 2048;      // chunks
 
 struct Aperture {
   double ct[3], rt;  // transmitter centre and radius
   double cr[3], rr;  // receiver centre and radius
 };
 
+// The aperture bounds of antennas [0, A), by all 256 threads of a block (fixed
+// reduction order, so every block that computes them gets the same bits); *out
+// is written by thread 0 and published by the closing barrier.
 template <typename T>
-__global__ void __launch_bounds__(256) aperture_kernel(const T* tx, const T* rx, int64_t A, Aperture* out) {
+__device__ void block_aperture(const T* tx, const T* rx, int64_t A, Aperture* out) {
   __shared__ double red[6][256];
   __shared__ double cen[6];
   const int tid = threadIdx.x;
   double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int64_t a = tid; a < A; a += blockDim.x) {
+  for (int64_t a = tid; a < A; a += 256) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       s[k] += static_cast<double>(ld_f(tx, a * 3 + k));
@@ -67,7 +76,7 @@ __global__ void __launch_bounds__(256) aperture_kernel(const T* tx, const T* rx,
   if (tid < 6) cen[tid] = A > 0 ? red[tid][0] / static_cast<double>(A) : NAN;
   __syncthreads();
   double mt = 0.0, mr = 0.0;
-  for (int64_t a = tid; a < A; a += blockDim.x) {
+  for (int64_t a = tid; a < A; a += 256) {
     double dt = 0.0, dr = 0.0;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -81,6 +90,7 @@ __global__ void __launch_bounds__(256) aperture_kernel(const T* tx, const T* rx,
     mt = fmax(mt, sqrt(dt));
     mr = fmax(mr, sqrt(dr));
   }
+  __syncthreads();  // red is reused
   red[0][tid] = mt;
   red[1][tid] = mr;
   __syncthreads();
@@ -103,6 +113,12 @@ __global__ void __launch_bounds__(256) aperture_kernel(const T* tx, const T* rx,
     out->rt = red[0][0] + 1e-12 * (red[0][0] + st);
     out->rr = red[1][0] + 1e-12 * (red[1][0] + sr);
   }
+  __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) aperture_kernel(const T* tx, const T* rx, int64_t A, Aperture* out) {
+  block_aperture(tx, rx, A, out);
 }
 
 __device__ __forceinline__ double dot3d(const double* a, const double* b) {
@@ -138,14 +154,18 @@ __device__ __forceinline__ bool culled_for_all(const Aperture& ap, const float* 
 }
 
 // Flag word w of chunk c covers points c*1024 + w*32 + lane; counts[c] is the
-// number of listed points of the chunk.
+// number of listed points of the chunk.  With a null `aperture` each block
+// bounds the antennas itself.
 template <typename T>
 __global__ void __launch_bounds__(kChunkThreads) point_flags_kernel(const T* normals, const T* points,
                                                                     const uint8_t* inb, int64_t P,
-                                                                    const Aperture* aperture,
-                                                                    uint32_t* words, int* counts) {
+                                                                    const Aperture* aperture, const T* tx,
+                                                                    const T* rx, int64_t A, uint32_t* words,
+                                                                    int* counts) {
   __shared__ int warp_count[kChunkThreads / 32];
-  const Aperture ap = *aperture;
+  __shared__ Aperture ap_s;
+  if (aperture == nullptr) block_aperture(tx, rx, A, &ap_s);
+  const Aperture ap = aperture != nullptr ? *aperture : ap_s;
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * kChunk;
@@ -215,17 +235,38 @@ __global__ void __launch_bounds__(1024) chunk_scan_kernel(const int* counts, int
 
 // Writes the listed point indices of each chunk in ascending order; with
 // gradient outputs, every unlisted point gets zero gradients (all antennas'
-// grad_sigmas, grad_normals and grad_points).
+// grad_sigmas, grad_normals and grad_points).  With a null `offsets` each block
+// sums the counts of the chunks before its own, and the last block writes the
+// total.
 template <typename T>
 __global__ void __launch_bounds__(kChunkThreads) point_scatter_kernel(const uint32_t* words, const int* offsets,
-                                                                      int64_t P, int* list, int64_t A,
-                                                                      T* g_sigmas, T* g_normals,
+                                                                      const int* counts, int64_t chunks,
+                                                                      int* total, int64_t P, int* list,
+                                                                      int64_t A, T* g_sigmas, T* g_normals,
                                                                       T* g_points) {
   __shared__ uint32_t w_s[32];
   __shared__ int pre_s[32];
+  __shared__ int part_s[kChunkThreads / 32];
+  __shared__ int off_s;
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int64_t chunk = blockIdx.x;
+  if (offsets == nullptr) {
+    int x = 0;
+    for (int64_t i = threadIdx.x; i < chunk; i += kChunkThreads) x += counts[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) part_s[warp] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int w = 0; w < kChunkThreads / 32; ++w) t += part_s[w];
+      off_s = t;
+      if (chunk == chunks - 1) *total = t + counts[chunk];
+    }
+  } else if (threadIdx.x == 0) {
+    off_s = offsets[chunk];
+  }
   if (warp == 0) {
     const uint32_t w = words[chunk * 32 + lane];
     const int c = __popc(w);
@@ -239,7 +280,7 @@ __global__ void __launch_bounds__(kChunkThreads) point_scatter_kernel(const uint
     pre_s[lane] = x - c;
   }
   __syncthreads();
-  const int off = offsets[chunk];
+  const int off = off_s;
   const T zero = from_f<T>(0.0f);
 #pragma unroll
   for (int k = 0; k < kChunk / kChunkThreads; ++k) {
@@ -298,13 +339,18 @@ cudaError_t launch_point_list(const TracerArgs& a, void* ws, bool zero_grads, cu
   int* total = reinterpret_cast<int*>(base + l.total);
   int* list = reinterpret_cast<int*>(base + l.list);
   const int64_t chunks = (a.P + kChunk - 1) / kChunk;
-  aperture_kernel<T><<<1, 256, 0, st>>>(static_cast<const T*>(a.tx), static_cast<const T*>(a.rx), a.A, ap);
+  const T* tx = static_cast<const T*>(a.tx);
+  const T* rx = static_cast<const T*>(a.rx);
+  const bool inline_aperture = a.A <= kInlineApertureMax;
+  const bool inline_scan = chunks <= kInlineScanMax;
+  if (!inline_aperture) aperture_kernel<T><<<1, 256, 0, st>>>(tx, rx, a.A, ap);
   point_flags_kernel<T><<<static_cast<unsigned>(chunks), kChunkThreads, 0, st>>>(
-      static_cast<const T*>(a.normals), static_cast<const T*>(a.points), a.inbounds, a.P, ap, words, counts);
-  chunk_scan_kernel<<<1, 1024, 0, st>>>(counts, chunks, offsets, total);
+      static_cast<const T*>(a.normals), static_cast<const T*>(a.points), a.inbounds, a.P,
+      inline_aperture ? nullptr : ap, tx, rx, a.A, words, counts);
+  if (!inline_scan) chunk_scan_kernel<<<1, 1024, 0, st>>>(counts, chunks, offsets, total);
   point_scatter_kernel<T><<<static_cast<unsigned>(chunks), kChunkThreads, 0, st>>>(
-      words, offsets, a.P, list, a.A, zero_grads ? static_cast<T*>(a.grad_sigmas) : nullptr,
-      zero_grads ? static_cast<T*>(a.grad_normals) : nullptr,
+      words, inline_scan ? nullptr : offsets, counts, chunks, total, a.P, list, a.A,
+      zero_grads ? static_cast<T*>(a.grad_sigmas) : nullptr, zero_grads ? static_cast<T*>(a.grad_normals) : nullptr,
       zero_grads ? static_cast<T*>(a.grad_points) : nullptr);
   return cudaGetLastError();
 }

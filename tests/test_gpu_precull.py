@@ -160,3 +160,37 @@ def test_precull_nufft_form(scene):
     assert (xr == 0).all() and (xi == 0).all()
     gn, gs, gp = tracer_backward(w, g.real.copy(), g.imag.copy(), "nufft")
     assert (gn == 0).all() and (gs == 0).all() and (gp == 0).all()
+
+
+def _synthetic(A, P, S, seed, spread=0.01):
+    """Random specular points at ~0.4 m in front of an array of A antennas;
+    normals mostly face the array."""
+    from benchkit import scenes
+
+    rng = np.random.default_rng(seed)
+    tx = rng.normal(0, spread, (A, 3)).astype(np.float32)
+    rx = (tx + rng.normal(0, spread / 2, (A, 3))).astype(np.float32)
+    pts = (np.array([0.0, 0.0, 0.4]) + rng.normal(0, 0.08, (P, 3))).astype(np.float32)
+    n = rng.normal(0, 1, (P, 3)) - 1.2 * pts / np.linalg.norm(pts, axis=1, keepdims=True)
+    n = (n / np.linalg.norm(n, axis=1, keepdims=True)).astype(np.float32)
+    ch = scenes.chirp(S)
+    return dict(normals=n, sigmas=rng.uniform(0.1, 1.0, (A, P)).astype(np.float32), points=pts, tx=tx, rx=rx,
+                inbounds=rng.uniform(size=P) < 0.9, S=S, fs=ch.adc_sample_rate, f0=770.0, As=ch.As_sci)
+
+
+@pytest.mark.parametrize("A,P,S", [(2100, 4096, 32), (4, 2_200_000, 16)], ids=["wide_aperture", "many_chunks"])
+def test_precull_one_block_kernels(cuda, A, P, S):
+    """Past 2048 antennas the aperture is bounded by its own one-block kernel, past
+    2048 chunks of 1024 points the chunk counts are scanned by one: the same
+    guarantees as the in-block forms (every clearly live pair kept, exact zeros
+    elsewhere, the IF within the MIXED bar of FP64)."""
+    w = _synthetic(A, P, S, 11)
+    live, dead = _clear_masks(w)
+    assert live.any() and (~live.any(0)).any()
+    g = wp.residual(A, S, 12)
+    gn, gs, gp = tracer_backward(w, g.real.copy(), g.imag.copy(), "mixed")
+    assert (gs[live] != 0).all() and (gs[dead] == 0).all()
+    assert (gn[dead.all(0)] == 0).all()
+    rows = np.arange(0, A, max(1, A // 4))
+    err = wp.tracer_forward_error(_c(tracer_forward(w, S, "mixed")), w, rows)
+    assert err < MIXED_TOL
