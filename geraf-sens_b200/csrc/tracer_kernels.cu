@@ -493,12 +493,13 @@ __global__ void __launch_bounds__(128) tracer_bwd_plain_kernel(const TrP<T> p) {
 // Q1 = sum_n n conj(g) zeta^n alongside (2 more).
 //
 // Culled pairs (back-facing or grazing, rho < 1e-6) skip all of that, so per
-// stage the block first lists its live (point, antenna) pairs and then deals
-// them out evenly over all threads: no lane idles beside a lane that works.
+// stage the block first lists the (point, antenna) pairs that the early test
+// cannot cull and then deals them out evenly over all threads, which form each
+// pair's exact geometry once: no lane idles beside a lane that works.
 // Each pair's normal / position contributions land in shared memory, and the
 // point's owner thread adds them up in antenna order -- the same sums, in the
 // same order, as one thread walking its point's antennas.  Six blocks are kept
-// resident per SM (80 registers, no spills): 1-6% faster than the five that 93
+// resident per SM (80 registers): 1-6% faster than the five that 93
 // registers allowed, measured on 64 antennas x 524288 points x 128 samples and
 // 128 antennas x 262144 points x 256 samples.
 template <typename T, bool WITH_POINTS>
@@ -566,18 +567,15 @@ __global__ void __launch_bounds__(128, 6) tracer_bwd_mixed_kernel(const TrP<T> p
     const int64_t a0 = a_begin + static_cast<int64_t>(t) * p.rows;
     const int rws = static_cast<int>(min(static_cast<int64_t>(p.rows), a_end - a0));
 
-    // 1. list the live pairs of the stage; dead pairs get zero gradients
+    // 1. list the stage's candidate pairs, those the early test cannot cull (the
+    //    exact geometry, formed once in step 2, decides them); the other pairs get
+    //    zero gradients here
     for (int r = 0; r < rws; ++r) {
       if (!inside) break;
       const float* ps = pos + (s * p.rows + r) * 6;
       const float txp[3] = {ps[0], ps[1], ps[2]};
       const float rxp[3] = {ps[3], ps[4], ps[5]};
-      bool live = false;
-      if (active && !surely_culled(txp, rxp, own_nrm, own_pt)) {
-        SpecGeom geo;
-        specular_geometry(txp, rxp, own_nrm, own_pt, geo);
-        live = !culled(geo);
-      }
+      const bool live = active && !surely_culled(txp, rxp, own_nrm, own_pt);
       if (live) {
         list[r * TILE + atomicAdd(&cnt[r], 1)] = threadIdx.x;
       } else {
@@ -588,7 +586,7 @@ __global__ void __launch_bounds__(128, 6) tracer_bwd_mixed_kernel(const TrP<T> p
     }
     __syncthreads();
 
-    // 2. every thread takes live pairs k = tid, tid + TILE, ... in (row, list) order
+    // 2. every thread takes candidate pairs k = tid, tid + TILE, ... in (row, list) order
     int total = 0;
     for (int r = 0; r < rws; ++r) total += cnt[r];
     int r_cur = 0, r_start = 0;
@@ -609,6 +607,12 @@ __global__ void __launch_bounds__(128, 6) tracer_bwd_mixed_kernel(const TrP<T> p
       const float rxp[3] = {ps[3], ps[4], ps[5]};
       SpecGeom geo;
       specular_geometry(txp, rxp, nrm, pt, geo);
+      if (culled(geo)) {
+        p.g_sigmas[a * p.P + pj] = from_f<T>(0.0f);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) contrib[(r * NC + c) * TILE + slot] = 0.0f;
+        continue;
+      }
       const double px = pt[0], py = pt[1], pz = pt[2];
       const PhaseCycles pc = path_cycles(ps[0] - px, ps[1] - py, ps[2] - pz, ps[3] - px,
                                          ps[4] - py, ps[5] - pz, p.k0, p.b0, p.k1, p.b1);
@@ -1113,14 +1117,12 @@ int tr_fwd_blocks_per_sm(const TracerArgs& a, const Tuning& t, int groups) {
 Tuning tracer_forward_resolve(const TracerArgs& a, const Tuning& req) {
   if (a.mode == kNufft) return tracer_nufft_forward_resolve(a, req);
   Tuning t = req;
-  // MIXED: 64-thread blocks of 8-sample chunks (measured on B200 for 64 antennas x
-  // 524288 points x 128 samples: 0.56 ms, against 0.70 ms with 16-sample chunks and
-  // 0.84 ms with 256 threads; 128 antennas x 262144 points x 256 samples: 0.69 ms
-  // against 0.76 ms).  Small blocks stall fewer warps at the per-tile compaction
-  // barriers, and short chunks hold fewer accumulators, so more blocks fit each SM
-  // to hide the latency of the per-point geometry.
+  // MIXED: 64-thread blocks of 16-sample chunks (measured on B200 for 64 antennas x
+  // 524288 points x 128 samples with the point pre-cull: 12% faster than 8-sample
+  // chunks, which led before it; 256-thread blocks are slower).  Small blocks stall
+  // fewer warps at the per-tile compaction barriers.
   if (t.threads != 64 && t.threads != 128 && t.threads != 256) t.threads = a.mode == kMixed ? 64 : 256;
-  if (t.chunk != 8 && t.chunk != 16 && t.chunk != 32) t.chunk = a.mode == kMixed ? 8 : 16;
+  if (t.chunk != 8 && t.chunk != 16 && t.chunk != 32) t.chunk = 16;
   if (t.items <= 0) t.items = 1;
   if (t.stage_rows <= 0) t.stage_rows = 8;
   if (a.mode == kPlain) {
@@ -1160,7 +1162,9 @@ Tuning tracer_backward_resolve(const TracerArgs& a, const Tuning& req) {
   Tuning t = req;
   if (t.threads != 64 && t.threads != 128) t.threads = 128;
   if (t.items <= 0) t.items = 1;
-  if (t.stage_rows <= 0) t.stage_rows = 8;
+  // MIXED: 4-antenna stages keep 6 blocks resident per SM (8 fit 4, by shared
+  // memory); 5% faster on 64 antennas x 524288 points x 128 samples
+  if (t.stage_rows <= 0) t.stage_rows = a.mode == kMixed ? 4 : 8;
   t.stage_rows = std::min(t.stage_rows, 64);
   if (t.chunk <= 0) t.chunk = 16;
   const int64_t rows_total = std::max<int64_t>(1, (a.A + t.stage_rows - 1) / t.stage_rows);
