@@ -329,6 +329,61 @@ __device__ __forceinline__ void rotate_accumulate(float2 s0, float2 z, float2 (&
   }
 }
 
+// Residual sums of the tracer adjoints for one (point, antenna) pair, from a
+// residual row g (real and imaginary parts, ld samples, ld a multiple of 4,
+// samples past S zero) in shared memory:
+//   Q  = sum_n conj(g_n) zeta^n,   Q1 = zeta Q'(zeta) = sum_n n conj(g_n) zeta^n.
+// Horner in w = zeta^2 on the even and odd samples at once, one chain per lane
+// of packed f32x2 operands.  The lanes carry the conjugates
+// E = sum_m g_2m conj(w)^m, O = sum_m g_2m+1 conj(w)^m (so no operand needs a
+// negation) and their derivatives E', O' in conj(w):
+//   conj(Q)  = E + conj(zeta) O,
+//   conj(Q1) = 2 conj(w) E' + conj(zeta) (2 conj(w) O' + O).
+// Per two samples: 4 fma.rn.f32x2 for (E, O), 4 more for (E', O') when Q1 is
+// wanted.
+template <bool WITH_Q1, typename R>
+__device__ __forceinline__ void residual_sums(const R* rowr, const R* rowi, int ld, float2 zt, float2& q,
+                                              float2& q1) {
+  const float2 wz = cmul(zt, zt);
+  const float2 wr2 = make_float2(wz.x, wz.x), wi2 = make_float2(wz.y, wz.y);
+  const float2 nwi2 = make_float2(-wz.y, -wz.y);
+  float2 pr = make_float2(0.0f, 0.0f), pim = make_float2(0.0f, 0.0f);  // (E, O) real, imaginary
+  float2 dr2 = make_float2(0.0f, 0.0f), di2 = make_float2(0.0f, 0.0f);  // (E', O')
+#pragma unroll 2
+  for (int n = ld - 4; n >= 0; n -= 4) {
+    const float4 a4 = lds4(rowr + n);
+    const float4 b4 = lds4(rowi + n);
+    const float2 gre[2] = {make_float2(a4.z, a4.w), make_float2(a4.x, a4.y)};
+    const float2 gim[2] = {make_float2(b4.z, b4.w), make_float2(b4.x, b4.y)};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (WITH_Q1) {  // D <- D conj(w) + P (P before its update)
+        const float2 ndr = ffma2(dr2, wr2, ffma2(di2, wi2, pr));
+        const float2 ndi = ffma2(di2, wr2, ffma2(dr2, nwi2, pim));
+        dr2 = ndr;
+        di2 = ndi;
+      }
+      // P <- P conj(w) + g
+      const float2 npr = ffma2(pr, wr2, ffma2(pim, wi2, gre[h]));
+      const float2 npi = ffma2(pim, wr2, ffma2(pr, nwi2, gim[h]));
+      pr = npr;
+      pim = npi;
+    }
+  }
+  const float2 zc = make_float2(zt.x, -zt.y);
+  const float2 qc = cmul(zc, make_float2(pr.y, pim.y));
+  q = make_float2(pr.x + qc.x, -(pim.x + qc.y));
+  if (WITH_Q1) {
+    const float2 wc = make_float2(wz.x, -wz.y);
+    const float2 de = cmul(wc, make_float2(dr2.x, di2.x));
+    const float2 dodd = cmul(wc, make_float2(dr2.y, di2.y));
+    const float2 t1 = cmul(zc, make_float2(2.0f * dodd.x + pr.y, 2.0f * dodd.y + pim.y));
+    q1 = make_float2(2.0f * de.x + t1.x, -(2.0f * de.y + t1.y));
+  } else {
+    q1 = make_float2(0.0f, 0.0f);
+  }
+}
+
 // Stages the tx and rx positions of `rws` antennas from a0 into slot `stage`
 // of a [2][rows_max][6] shared table, as PosT (float or double).
 template <typename T, typename PosT>

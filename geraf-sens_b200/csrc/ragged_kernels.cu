@@ -282,9 +282,10 @@ __device__ __forceinline__ int64_t point_antenna(const int64_t* offsets, int64_t
   return lo;
 }
 
-// Gradients of one live (uncut, in-bounds) point pi of antenna a.  The residual
-// row comes from shared memory (rr, ri: ld floats each) or, when rr is null,
-// from global memory.
+// Gradients of one in-bounds point pi of antenna a that the early test cannot
+// cull (zeros when its exact geometry culls it).  The residual row comes from
+// shared memory (rr, ri: ld floats each) or, when rr is null, from global
+// memory.
 template <typename T, bool WITH_POINTS>
 __device__ __forceinline__ void ragged_point_grads(const RgP<T>& p, int64_t pi, int64_t a, const float* rr,
                                                    const float* ri, int ld) {
@@ -295,11 +296,22 @@ __device__ __forceinline__ void ragged_point_grads(const RgP<T>& p, int64_t pi, 
   ld3(p.rx, a, rxp);
   SpecGeom geo;
   specular_geometry(txp, rxp, nrm, pt, geo);
+  if (culled(geo)) {  // a candidate the exact geometry culls
+    p.g_sigmas[pi] = from_f<T>(0.0f);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) p.g_normals[pi * 3 + q] = from_f<T>(0.0f);
+    if (WITH_POINTS) {
+#pragma unroll
+      for (int q = 0; q < 3; ++q) p.g_points[pi * 3 + q] = from_f<T>(0.0f);
+    }
+    return;
+  }
   const double px = pt[0], py = pt[1], pz = pt[2];
   const PhaseCycles pc = path_cycles(txp[0] - px, txp[1] - py, txp[2] - pz, rxp[0] - px, rxp[1] - py,
                                      rxp[2] - pz, p.k0, p.b0, p.k1, p.b1);
   const float2 zt = cis_cycles(pc.dcyc);
   float qr = 0.0f, qi = 0.0f, dr = 0.0f, di = 0.0f;
+  float2 q1 = make_float2(0.0f, 0.0f);
   auto step = [&](float cr, float ci) {
     if (WITH_POINTS) {
       const float ndr = fmaf(dr, zt.x, fmaf(-di, zt.y, qr));
@@ -313,16 +325,15 @@ __device__ __forceinline__ void ragged_point_grads(const RgP<T>& p, int64_t pi, 
     qi = nqi;
   };
   if (rr != nullptr) {
-    for (int n = ld - 4; n >= 0; n -= 4) {
-      const float4 x = lds4(rr + n);
-      const float4 y = lds4(ri + n);
-      step(x.w, y.w);
-      step(x.z, y.z);
-      step(x.y, y.y);
-      step(x.x, y.x);
-    }
+    // staged row: packed even/odd Horner in zeta^2
+    float2 qv;
+    residual_sums<WITH_POINTS>(rr, ri, ld, zt, qv, q1);
+    qr = qv.x;
+    qi = qv.y;
   } else {
+    // row read from global memory: scalar Horner, Q1 = zeta Q'(zeta) from its derivative chain
     for (int64_t n = p.S - 1; n >= 0; --n) step(ld_f(p.gr, a * p.S + n), ld_f(p.gi, a * p.S + n));
+    q1 = cmul(zt, make_float2(dr, di));
   }
   const float inv_pa = 1.0f / static_cast<float>(p.offsets[a + 1] - p.offsets[a]);
   const float2 e0 = cis_cycles(pc.frac0);
@@ -339,7 +350,6 @@ __device__ __forceinline__ void ragged_point_grads(const RgP<T>& p, int64_t pi, 
   if (WITH_POINTS) {
     const float w0 = static_cast<float>(2.0 * static_cast<double>(kPiF) * p.f0);
     const float w1s = static_cast<float>(2.0 * static_cast<double>(kPiF) * p.As / p.fs);
-    const float2 q1 = cmul(zt, make_float2(dr, di));
     const float2 f = cmul(e0, make_float2(w0 * qr + w1s * q1.x, w0 * qi + w1s * q1.y));
     const float amp = sigma_value * geo.align * atten;
     const float d_tau = -amp * f.y;
@@ -357,10 +367,11 @@ __device__ __forceinline__ void ragged_point_grads(const RgP<T>& p, int64_t pi, 
 }
 
 // Adjoint.  A block screens kBwdTile consecutive points, kBwdCand per thread:
-// it finds each point's antenna, culls it by the specular geometry, and writes
-// zero gradients for culled, out-of-bounds and unowned points; the live points
-// are listed in shared memory and then dealt out over the block, so every lane
-// runs the full sample recurrence of a live point.  (About 60% of a typical
+// it finds each point's antenna, applies the early cull test, and writes zero
+// gradients for culled, out-of-bounds and unowned points; the other points are
+// listed in shared memory and then dealt out over the block, so every lane forms
+// a listed point's exact geometry and, unless that culls it, runs its full
+// sample recurrence (packed even/odd Horner, residual_sums).  (About 60% of a typical
 // step's points are live; with one point per thread 40% of the lanes would sit
 // out the recurrence.)  A point's gradients depend on that point only, so the
 // results do not depend on the list order.  Residual rows of the antennas the
@@ -399,11 +410,8 @@ __global__ void __launch_bounds__(kBwdThreads) ragged_bwd_kernel(const RgP<T> p,
         ld3(p.points, pi, pt);
         ld3(p.tx, a, txp);
         ld3(p.rx, a, rxp);
-        if (!surely_culled(txp, rxp, nrm, pt)) {
-          SpecGeom geo;
-          specular_geometry(txp, rxp, nrm, pt, geo);
-          live = !culled(geo);
-        }
+        // a candidate: the exact geometry, formed once when its gradients are, decides it
+        live = !surely_culled(txp, rxp, nrm, pt);
       }
       if (!live) {
         p.g_sigmas[pi] = from_f<T>(0.0f);

@@ -619,43 +619,9 @@ __global__ void __launch_bounds__(128, 6) tracer_bwd_mixed_kernel(const TrP<T> p
       const float2 zt = cis_cycles(pc.dcyc);
       const T* rowr = stg.stage_ptr(s, 0) + r * p.ld;
       const T* rowi = stg.stage_ptr(s, 1) + r * p.ld;
-      // Q = sum_n conj(g_n) zeta^n and Q1 = zeta Q'(zeta) by Horner in w = zeta^2 on the
-      // even and odd samples at once, packed in the two lanes of f32x2 operands.
-      // The lanes carry the conjugates E = sum_m g_2m conj(w)^m, O = sum_m g_2m+1 conj(w)^m
-      // (so no operand needs a negation) and their derivatives E', O' in conj(w):
-      //   conj(Q)  = E + conj(zeta) O,
-      //   conj(Q1) = 2 conj(w) E' + conj(zeta) (2 conj(w) O' + O).
-      // Per two samples: 4 fma.rn.f32x2 for (E, O), 4 more for (E', O').
-      const float2 wz = cmul(zt, zt);
-      const float2 wr2 = make_float2(wz.x, wz.x), wi2 = make_float2(wz.y, wz.y);
-      const float2 nwi2 = make_float2(-wz.y, -wz.y);
-      float2 pr = make_float2(0.0f, 0.0f), pim = make_float2(0.0f, 0.0f);  // (E, O) real, imaginary
-      float2 dr2 = make_float2(0.0f, 0.0f), di2 = make_float2(0.0f, 0.0f);  // (E', O')
-#pragma unroll 2
-      for (int n = p.ld - 4; n >= 0; n -= 4) {
-        const float4 a4 = lds4(rowr + n);
-        const float4 b4 = lds4(rowi + n);
-        const float2 gre[2] = {make_float2(a4.z, a4.w), make_float2(a4.x, a4.y)};
-        const float2 gim[2] = {make_float2(b4.z, b4.w), make_float2(b4.x, b4.y)};
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          if (WITH_POINTS) {  // D <- D conj(w) + P (P before its update)
-            const float2 ndr = ffma2(dr2, wr2, ffma2(di2, wi2, pr));
-            const float2 ndi = ffma2(di2, wr2, ffma2(dr2, nwi2, pim));
-            dr2 = ndr;
-            di2 = ndi;
-          }
-          // P <- P conj(w) + g
-          const float2 npr = ffma2(pr, wr2, ffma2(pim, wi2, gre[h]));
-          const float2 npi = ffma2(pim, wr2, ffma2(pr, nwi2, gim[h]));
-          pr = npr;
-          pim = npi;
-        }
-      }
-      const float2 zc = make_float2(zt.x, -zt.y);
-      const float2 qc = cmul(zc, make_float2(pr.y, pim.y));
-      const float qr = pr.x + qc.x;
-      const float qi = -(pim.x + qc.y);
+      float2 qv, q1;  // Q and Q1 = zeta Q'(zeta): packed even/odd Horner in zeta^2
+      residual_sums<WITH_POINTS>(rowr, rowi, p.ld, zt, qv, q1);
+      const float qr = qv.x, qi = qv.y;
       const float2 e0 = cis_cycles_fast(pc.frac0);
       const float2 eq = cmul(e0, make_float2(qr, qi));
       // sum_n (g_r cos + g_i sin) = Re(exp(j phi0) Q)
@@ -672,11 +638,6 @@ __global__ void __launch_bounds__(128, 6) tracer_bwd_mixed_kernel(const TrP<T> p
       for (int c = 0; c < 3; ++c) contrib[(r * NC + c) * TILE + slot] = normal_scale * gsa[c] * sum_re;
       if (WITH_POINTS) {
         // sum_n w_n (g_i cos - g_r sin) = -Im(exp(j phi0) (w0 Q + w1s Q1))
-        const float2 wc = make_float2(wz.x, -wz.y);
-        const float2 de = cmul(wc, make_float2(dr2.x, di2.x));
-        const float2 dodd = cmul(wc, make_float2(dr2.y, di2.y));
-        const float2 t1 = cmul(zc, make_float2(2.0f * dodd.x + pr.y, 2.0f * dodd.y + pim.y));
-        const float2 q1 = make_float2(2.0f * de.x + t1.x, -(2.0f * de.y + t1.y));
         const float2 f = cmul(e0, make_float2(w0 * qr + w1s * q1.x, w0 * qi + w1s * q1.y));
         const float amp = sigma_value * geo.align * propagation_attenuation;
         const float d_tau = -amp * f.y;
