@@ -18,7 +18,8 @@
  *     stream) and the call returns without synchronising.
  *   - Return value: GERAF_OK, or a GERAF_ERR_* code; `geraf_rf_last_error()`
  *     then holds a message for the calling thread.
- *   - Entry points that may use a reduction workspace take `workspace` /
+ *   - Entry points that may use a workspace (reduction partials, the tracer's
+ *     point list) take `workspace` /
  *     `workspace_bytes`; the matching `*_workspace_bytes` query returns the
  *     size needed for the same arguments (0 when none is needed, in which case
  *     `workspace` may be NULL).  A workspace must be 256-byte aligned device
@@ -179,6 +180,10 @@ int32_t geraf_mf_forward_noalloc(const void* real, const void* imag, const void*
  * culled when rho < 1e-6 or i.n > 0; D = |tx_a - p| + |rx_a - p|; tau = (D + 0.15)/2.9979.
  * normals, points: [P,3]; sigmas: [A,P]; tx_pos, rx_pos: [A,3]; inbounds: [P] (u8);
  * output_real, output_imag: [A,S].
+ * In MIXED and NUFFT mode the forward and the adjoint first list, in their
+ * workspace (about 4.3 bytes per point), the in-bounds points that a
+ * conservative test cannot cull for every antenna of the call, and visit only
+ * those; the workspace is therefore needed even without split partials.
  * Replaces SignalTracer::SignalTracer_forward
  * (geraf/ops/RFSignalTracer/csrc/signal_tracer/SignalTracer_cuda.cu:314-356,
  *  kernel SignalTracer_cuda_kernel.cu:351-450). */
