@@ -177,6 +177,9 @@ def train(precision: str, graph: bool, steps: int, volume, half: float, power: f
             "final_chamfer_m": curve[-1][1]}
 
 
+CHAMFER_TOL = 0.05
+
+
 def compare(steps: int = 200, seed: int = 0, checkpoints: int = 8) -> dict:
     from .stage1 import Stage1RFStep
 
@@ -189,18 +192,31 @@ def compare(steps: int = 200, seed: int = 0, checkpoints: int = 8) -> dict:
     ref = train("plain", False, steps, volume, half, power, seed, checkpoints)
     target = ref["final_chamfer_m"]
     reach = next((k for k, c in fast["chamfer_m"] if k > 0 and c <= target), None)
+    # Equal error within the spread of the final Chamfer distance between
+    # numerically equivalent forms (the training is sensitive to the last bits of
+    # the sums): the first checkpoint within CHAMFER_TOL of PLAIN's final value.
+    reach_tol = next((k for k, c in fast["chamfer_m"] if k > 0 and c <= target * (1.0 + CHAMFER_TOL)), None)
+
+    def tail_mean(run):
+        last = [c for _, c in run["chamfer_m"][-3:]]
+        return sum(last) / len(last)
+
     out = {"workload": ("stage-1 RF step, 128 antennas x 2048 rays x 128 target samples (64 coarse), S = 256, "
                         "MF at the target points, target |MF| of the shell + torus scene (49152 channels, 128^3)"),
            "power": power, "mixed_graph": fast, "plain_eager": ref,
            "speedup_at_equal_steps": fast["it_per_s"] / ref["it_per_s"],
            "plain_final_chamfer_m": target,
-           "mixed_steps_to_plain_final_chamfer": reach}
-    if reach is not None:
-        t_fast = reach * fast["ms_per_step"] * 1e-3
-        t_ref = steps * ref["ms_per_step"] * 1e-3
-        out["mixed_seconds_to_plain_final_chamfer"] = t_fast
-        out["plain_seconds"] = t_ref
-        out["speedup_at_equal_chamfer"] = t_ref / t_fast
+           "last3_mean_chamfer_m": {"mixed_graph": tail_mean(fast), "plain_eager": tail_mean(ref)},
+           "mixed_steps_to_plain_final_chamfer": reach,
+           "chamfer_tolerance": CHAMFER_TOL,
+           "mixed_steps_to_plain_final_chamfer_within_tolerance": reach_tol}
+    t_ref = steps * ref["ms_per_step"] * 1e-3
+    out["plain_seconds"] = t_ref
+    for key, k in (("", reach), ("_within_tolerance", reach_tol)):
+        if k is not None:
+            t_fast = k * fast["ms_per_step"] * 1e-3
+            out["mixed_seconds_to_plain_final_chamfer" + key] = t_fast
+            out["speedup_at_equal_chamfer" + key] = t_ref / t_fast
     return out
 
 
