@@ -311,22 +311,43 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 // the recurrence grow at most ~m^2 eps (theta near 0 or pi) and ~m eps /
 // |sin theta| otherwise, which is why callers re-seed from exact phasors
 // every K samples.
-template <int K>
+// ASSIGN: acc is set to this term's samples instead of added to (the first term
+// of a tile), which spares zeroing the accumulators between tiles.
+template <int K, bool ASSIGN = false>
 __device__ __forceinline__ void rotate_accumulate(float2 s0, float2 z, float2 (&acc)[K]) {
   static_assert(K >= 2, "the recurrence needs two seeds");
   const float2 c2 = make_float2(2.0f * z.x, 2.0f * z.x);
   const float2 nc2 = make_float2(-2.0f * z.x, -2.0f * z.x);
+  const float2 zero = make_float2(0.0f, 0.0f);
   float2 xm1 = s0;
   float2 x = cmul(s0, z);
-  acc[0] = fadd2(acc[0], xm1);
-  acc[1] = fadd2(acc[1], x);
+  acc[0] = ASSIGN ? xm1 : fadd2(acc[0], xm1);
+  acc[1] = ASSIGN ? x : fadd2(acc[1], x);
 #pragma unroll
   for (int m = 2; m < K; ++m) {
     const float2 xn = ffma2((m & 1) ? c2 : nc2, x, xm1);
     xm1 = x;
     x = xn;
-    acc[m] = (m & 2) ? fsub2(acc[m], x) : fadd2(acc[m], x);
+    if (ASSIGN) acc[m] = (m & 2) ? fsub2(zero, x) : x;
+    else acc[m] = (m & 2) ? fsub2(acc[m], x) : fadd2(acc[m], x);
   }
+}
+
+// One tile of a sample-major kernel for lane l of L: acc = the sum over the
+// tile's terms vl = l, l + L, ... < count of rotate_accumulate, each term from
+// its seed and rotator (the first term assigns, so acc needs no zeroing).
+template <int K>
+__device__ __forceinline__ void rotate_tile(const float2* seeds, const float2* zeta, int l, int L, int count,
+                                            float2 (&acc)[K]) {
+  int vl = l;
+  if (vl < count) {
+    rotate_accumulate<K, true>(seeds[vl], zeta[vl], acc);
+    vl += L;
+  } else {
+#pragma unroll
+    for (int m = 0; m < K; ++m) acc[m] = make_float2(0.0f, 0.0f);
+  }
+  for (; vl < count; vl += L) rotate_accumulate<K>(seeds[vl], zeta[vl], acc);
 }
 
 // Residual sums of the tracer adjoints for one (point, antenna) pair, from a

@@ -451,12 +451,9 @@ __global__ void __launch_bounds__(256) mf_bwd_mixed_kernel(const MfBwdP<T> p) {
     __syncthreads();
     {  // phase 2
       const int count = static_cast<int>(min(static_cast<int64_t>(TILE), v_end - v0));
-      for (int vl = l; vl < count; vl += L) rotate_accumulate<K>(seeds[g * TILE + vl], zeta[vl], acc);
+      rotate_tile<K>(seeds + g * TILE, zeta, l, L, count, acc);
 #pragma unroll
-      for (int m = 0; m < K; ++m) {
-        hi[m] = fadd2(hi[m], acc[m]);
-        acc[m] = make_float2(0.0f, 0.0f);
-      }
+      for (int m = 0; m < K; ++m) hi[m] = fadd2(hi[m], acc[m]);
     }
     __syncthreads();
   }

@@ -222,12 +222,9 @@ __global__ void __launch_bounds__(256) ragged_fwd_kernel(const RgP<T> p) {
       }
       load_point(p0 + TILE + threadIdx.x);  // in flight during the sums below
       __syncthreads();
-      for (int vl = l; vl < count; vl += L) rotate_accumulate<K>(seeds[g * TILE + vl], zeta[vl], acc);
+      rotate_tile<K>(seeds + g * TILE, zeta, l, L, count, acc);
 #pragma unroll
-      for (int m = 0; m < K; ++m) {
-        hi[m] = fadd2(hi[m], acc[m]);
-        acc[m] = make_float2(0.0f, 0.0f);
-      }
+      for (int m = 0; m < K; ++m) hi[m] = fadd2(hi[m], acc[m]);
       __syncthreads();
     }
     // Reduce the lanes of each sample group and store this item's partial row.
