@@ -59,6 +59,8 @@ def parse_args(argv=None):
                     help="comma list of secondary measurements: plain, adjoint, nufft, tracer, "
                          "ragged, stage1, cpu")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--ragged-antennas", type=int, default=256,
+                    help="antennas of the ragged-step extra (fewer for a small profiling case)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--stage1-steps", type=int, default=160,
                     help="training steps per form of the stage-1 equal-error comparison")
@@ -496,7 +498,7 @@ def _ragged_extra(args, dev) -> dict:
     from geraf_b200 import autotune
     from geraf_b200.step import RaggedRFStep
 
-    w = ragged_workload(dev, args.seed)
+    w = ragged_workload(dev, args.seed, num_antennas=args.ragged_antennas)
     ch = scenes.chirp(w["S"])
     cfg = ch.radar_cfg(fc_start=770.0)
     vox = torch.tensor(scenes.voxel_grid(64, size=0.32).T.copy(), device=dev)

@@ -384,22 +384,28 @@ __global__ void __launch_bounds__(kBwdThreads) ragged_bwd_kernel(const RgP<T> p,
   __shared__ int s_live[kBwdTile];
   __shared__ int s_nlive;
   __shared__ long long s_a0, s_a1;
+  __shared__ int s_single;
   const int64_t base = blockIdx.x * static_cast<int64_t>(kBwdTile);
   const int lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    bool owned;
+    bool owned0, owned1;
     s_nlive = 0;
-    s_a0 = point_antenna(p.offsets, p.A, base, &owned);
-    s_a1 = point_antenna(p.offsets, p.A, min(p.P, base + kBwdTile) - 1, &owned);
+    s_a0 = point_antenna(p.offsets, p.A, base, &owned0);
+    s_a1 = point_antenna(p.offsets, p.A, min(p.P, base + kBwdTile) - 1, &owned1);
+    // Both ends owned by one antenna: with offsets[a] <= first <= pi <= last <
+    // offsets[a + 1], that antenna owns every point between, no search needed.
+    s_single = owned0 && owned1 && s_a0 == s_a1;
   }
   __syncthreads();
+  const bool single = s_single != 0;
+  const int64_t a_single = s_a0;
   for (int k = 0; k < kBwdCand; ++k) {
     const int c = threadIdx.x + k * kBwdThreads;
     const int64_t pi = base + c;
     bool live = false;
     if (pi < p.P) {
-      bool owned;
-      const int64_t a = point_antenna(p.offsets, p.A, pi, &owned);
+      bool owned = true;
+      const int64_t a = single ? a_single : point_antenna(p.offsets, p.A, pi, &owned);
       if (!owned && p.status != nullptr) atomicExch(p.status, kStatusBadOffsets);
       if (owned && (p.inb == nullptr || p.inb[pi])) {
         float nrm[3], pt[3], txp[3], rxp[3];
@@ -449,7 +455,7 @@ __global__ void __launch_bounds__(kBwdThreads) ragged_bwd_kernel(const RgP<T> p,
   for (int i = threadIdx.x; i < nlive; i += kBwdThreads) {
     const int64_t pi = base + s_live[i];
     bool owned;
-    const int64_t a = point_antenna(p.offsets, p.A, pi, &owned);
+    const int64_t a = single ? a_single : point_antenna(p.offsets, p.A, pi, &owned);
     // A row outside the staged span (possible only with non-monotonic offsets) is read from global memory.
     const bool row_staged = staged && a >= a0 && a <= a1;
     const float* rr = row_staged ? srow + ((a - a0) * 2 + 0) * ld : nullptr;
