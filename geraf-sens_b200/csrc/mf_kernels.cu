@@ -158,15 +158,23 @@ __global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
       }
     }
     __syncthreads();
-    constexpr int B = 64;  // samples per Goertzel block
-    // z^B is raised to at most nb - 1 powers; up to 8 blocks its hardware phasor
-    // is accurate enough (phase error <= 8 x 4e-7 rad)
-    const bool few_blocks = (p.ld + B - 1) / B <= kFastPowers;
+    // The recurrence restarts every B = 64 samples, or every 2B for a voxel whose
+    // |sin theta| >= 0.1: its rounding errors grow at most ~m eps / |sin theta|
+    // over m samples, so 128 samples keep them below ~1e-4 relative even in the
+    // worst case at |sin theta| = 0.1 (measured ~5e-7 on the 49152 x 256 x 128^3
+    // workload, where theta is 0.2 to 0.4 rad), and only near theta = 0 or pi do
+    // the shorter blocks matter.  The longer blocks halve the block extractions.
+    constexpr int B = 64;
+    // z^B and z^2B are raised to at most nb - 1 powers; up to 8 blocks their
+    // hardware phasors are accurate enough (phase error <= 8 x 4e-7 rad)
+    const int nb = (p.ld + B - 1) / B;
+    const bool few_blocks = nb <= kFastPowers;
     for (int r = 0; r < rws; ++r) {
       const double* ps = pos + (s * p.rows + r) * 6;
       const double tx = ps[0], ty = ps[1], tz = ps[2], rx = ps[3], ry = ps[4], rz = ps[5];
       float frac0[VPT], sn[VPT];
       float2 C2[VPT], ZB[VPT], R[VPT];
+      unsigned long_blocks = 0;  // bit j: voxel j restarts every 2B samples
 #pragma unroll
       for (int j = 0; j < VPT; ++j) {
         const double dx = static_cast<double>(vx[j]), dy = static_cast<double>(vy[j]),
@@ -177,19 +185,20 @@ __global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
         frac0[j] = pc.frac0;
         C2[j] = make_float2(2.0f * c1.x, 2.0f * c1.x);
         sn[j] = c1.y;
-        const float kb = pc.dcyc * static_cast<float>(B);
+        const bool lng = fabsf(c1.y) >= 0.1f;
+        long_blocks |= lng ? (1u << j) : 0u;
+        // the multiplier of a block of this voxel's length: z^2B or z^B
+        const float kb = pc.dcyc * static_cast<float>(lng ? 2 * B : B);
         const float2 zb = few_blocks ? cis_cycles_fast(kb - rintf(kb)) : cis_cycles(kb - rintf(kb));
-        ZB[j] = make_float2(zb.x, -zb.y);  // z^B
+        ZB[j] = make_float2(zb.x, -zb.y);
         R[j] = make_float2(0.0f, 0.0f);
       }
       const float2* row = dup + r * p.ld;
-      const int nb = (p.ld + B - 1) / B;
-      for (int blk = nb - 1; blk >= 0; --blk) {
-        const int lo = blk * B;
-        const int hi = min(p.ld, lo + B);
-        float2 b1[VPT], b2[VPT];
+      float2 b1[VPT], b2[VPT];
 #pragma unroll
-        for (int j = 0; j < VPT; ++j) b1[j] = b2[j] = make_float2(0.0f, 0.0f);
+      for (int j = 0; j < VPT; ++j) b1[j] = b2[j] = make_float2(0.0f, 0.0f);
+      // The recurrence over samples [lo, hi), from the highest down.
+      auto recur = [&](int lo, int hi) {
 #pragma unroll 2
         for (int n = hi - 2; n >= lo; n -= 2) {
           const float4 a = *reinterpret_cast<const float4*>(row + n);  // (x_n, x_n+1)
@@ -207,14 +216,34 @@ __global__ void __launch_bounds__(256) mf_fwd_mixed_kernel(const MfFwdP<T> p) {
             b1[j] = ffma2(C2[j], b1[j], t);
           }
         }
+      };
+      // Voxel j's block ends: its sum b1 - exp(j theta) b2 enters the Horner over
+      // blocks, R <- R z^len + block sum, and the recurrence restarts.  (The first
+      // block from the top may be shorter; R is still zero then.)
+      auto end_block = [&](int j) {
+        const float2 e = make_float2(0.5f * C2[j].x, sn[j]);
+        const float2 eb = cmul(e, b2[j]);
+        const float2 pb = make_float2(b1[j].x - eb.x, b1[j].y - eb.y);
+        const float2 rz = cmul(R[j], ZB[j]);
+        R[j] = make_float2(rz.x + pb.x, rz.y + pb.y);
+        b1[j] = b2[j] = make_float2(0.0f, 0.0f);
+      };
+      if (!__any_sync(0xffffffffu, (~long_blocks & ((1u << VPT) - 1u)) != 0u)) {
+        // every voxel of the warp has 2B-sample blocks (the usual case)
+        for (int lo = ((nb - 1) >> 1) * 2 * B; lo >= 0; lo -= 2 * B) {
+          recur(lo, min(p.ld, lo + 2 * B));
 #pragma unroll
-        for (int j = 0; j < VPT; ++j) {
-          // block sum b1 - exp(j theta) b2, then Horner over blocks in z^B
-          const float2 e = make_float2(0.5f * C2[j].x, sn[j]);
-          const float2 eb = cmul(e, b2[j]);
-          const float2 pb = make_float2(b1[j].x - eb.x, b1[j].y - eb.y);
-          const float2 rz = cmul(R[j], ZB[j]);
-          R[j] = make_float2(rz.x + pb.x, rz.y + pb.y);
+          for (int j = 0; j < VPT; ++j) end_block(j);
+        }
+      } else {
+        // B-sample steps; a voxel with long blocks ends one at every second step
+        for (int blk = nb - 1; blk >= 0; --blk) {
+          recur(blk * B, min(p.ld, blk * B + B));
+          const bool even = (blk & 1) == 0;
+#pragma unroll
+          for (int j = 0; j < VPT; ++j) {
+            if (even || !((long_blocks >> j) & 1u)) end_block(j);
+          }
         }
       }
 #pragma unroll

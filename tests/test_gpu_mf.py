@@ -298,3 +298,27 @@ def test_mixed_long_rows_vs_fp64(cuda, S):
         hr, hi = mf_backward(gr, gi, c["tx"], c["rx"], c["vox"], A, S, ch.adc_sample_rate, ch.As_sci, "mixed",
                              tuning=tun)
         assert rel_l2(hr + 1j * hi, bref[0] + 1j * bref[1]) < 1e-5, tun
+
+
+def test_mixed_near_field_block_lengths_vs_fp64(cuda):
+    """Voxels 1 cm to 30 cm in front of the array at the 256-sample chirp: the
+    per-sample phase step theta runs from about 0.05 to 0.25 rad, so the forward's
+    voxels restart their recurrence every 64 samples (|sin theta| < 0.1, the near
+    ones) or every 128 (the rest), both within the same launch and thread."""
+    rng = np.random.default_rng(9)
+    tx, rx = scenes.virtual_array(2)
+    ch = scenes.chirp(256)
+    pos = np.stack([rng.uniform(-0.04, 0.04, 12), rng.uniform(-0.04, 0.04, 12), rng.uniform(0.02, 0.28, 12)], 1)
+    amp = rng.standard_normal(12) + 1j * rng.standard_normal(12)
+    re, im = scenes.synthesize_if_numpy(tx, rx, pos, amp, ch, snr_db=20.0, rng=rng)
+    g = np.linspace(-0.05, 0.05, 6)
+    z = np.linspace(0.01, 0.30, 24)
+    vx, vy, vz = np.meshgrid(g, g, z, indexing="ij")
+    vox = np.stack([vx.ravel(), vy.ravel(), vz.ravel()]).astype(np.float32)
+    d = (np.linalg.norm(tx[:, None, :] - vox.T[None], axis=2) + np.linalg.norm(rx[:, None, :] - vox.T[None], axis=2))
+    k1 = (np.float32(np.pi) / np.pi) * ch.As_sci / (ch.adc_sample_rate * 2.9979)
+    sin_theta = np.abs(np.sin(2 * np.pi * (d + 0.15) * k1))
+    assert (sin_theta < 0.1).any() and (sin_theta >= 0.1).any()
+    ref = orc.mf_forward(re, im, tx, rx, vox, ch.adc_sample_rate, ch.As_sci)
+    mr, mi = mf_forward(re, im, tx, rx, vox, ch.adc_sample_rate, ch.As_sci, "mixed")
+    assert rel_l2(mr + 1j * mi, ref[0] + 1j * ref[1]) < 1e-5
