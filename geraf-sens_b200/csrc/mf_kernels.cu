@@ -15,7 +15,7 @@
 // MIXED kernels use that phi is linear in n: with z = exp(-j 2 pi dcyc) the
 // forward inner sum is exp(-j phi0) * P_a(z), P_a(z) = sum_n s[a,n] z^n,
 // evaluated by a second-order (Goertzel) recurrence on packed complex samples
-// in 64-sample blocks; the adjoint generates
+// in 128- or 64-sample blocks; the adjoint generates
 // G[v] exp(j phi0) zeta^n by a three-term recurrence per real component,
 // re-seeded from exact phasors every K samples.  phi0 is reduced modulo one
 // cycle in FP64 (path_cycles), so only two phasors per (v, a) are evaluated.
@@ -85,8 +85,9 @@ __device__ __forceinline__ float sq(float x) { return x * x; }
 //   b_n = x_n + 2 cos(theta) b_{n+1} - b_{n+2}    (one sub.f32x2 + one fma.f32x2)
 // so that sum_{n in block} x_n z^(n - lo) = b_lo - exp(j theta) b_{lo+1}, since
 // z^m = U_m(cos theta) - exp(j theta) U_{m-1}(cos theta) (Chebyshev polynomials of
-// the second kind).  The recurrence restarts every B = 64 samples, which bounds
-// its error growth, and the block sums are combined by Horner in z^B.  Per
+// the second kind).  The recurrence restarts every 128 samples (64 where
+// |sin theta| < 0.1), which bounds its error growth, and the block sums are
+// combined by Horner in z^128 (z^64).  Per
 // voxel-sample this is 2 issue slots and 4 FP32 lane-operations, like the
 // packed complex Horner step it replaces, but the sample operand is shared by
 // all the thread's voxels and the coefficient is real: the loop alone runs
