@@ -967,7 +967,7 @@ Tuning mf_forward_resolve(const MfArgs& a, const Tuning& req) {
     if (a.mode == kMixed) {
       // Enough splits that one split's IF rows (streamed by every block resident
       // at the same time, the blocks being split-major) stay within 32 MiB of L2:
-      // 4 splits of 25 MB for 49152 x 256 samples.  The split count changes the
+      // 3 splits of 32 MiB for 49152 x 256 samples.  The split count changes the
       // kernel's time by under 0.3% (measured 1 to 6 on B200); the partial sums
       // cost one pass over splits x N x 8 bytes.
       const int64_t if_bytes = 2 * a.A * a.S * static_cast<int64_t>(elem_size(a.dtype));
