@@ -241,7 +241,7 @@ __device__ __forceinline__ float2 cis_cycles(float x) {
 // e^{j 2 pi x} for |x| <= 1/2 from the hardware sine and cosine (__sincosf,
 // absolute error ~4e-7 on [-pi, pi]): for the phasor that multiplies a term
 // once (its carrier or start phase), and for a rotator raised to at most
-// kFastPowers powers (per 64-sample block, per sample group), whose phase error
+// kFastPowers powers (per sample block, per sample group), whose phase error
 // then stays below ~3e-6 rad, far inside the MIXED form's bound.  The
 // per-sample rotators, and block or group rotators of longer rows, keep
 // cis_cycles: their error grows with the steps they take.

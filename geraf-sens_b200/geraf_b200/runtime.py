@@ -33,7 +33,7 @@ _MODES = {"mixed": _lib.MODE_MIXED, "plain": _lib.MODE_PLAIN, "nufft": _lib.MODE
 def default_precision() -> str:
     """Arithmetic form used when a call does not name one.
 
-    ``mixed`` (FP64 phase reduction, Horner / rotator phasors, compensated
+    ``mixed`` (FP64 phase reduction, recurrence sample sums, compensated
     sums; checked against an FP64 oracle) unless ``GERAF_RF_PRECISION`` names
     ``plain`` (the reference's FP32 arithmetic, expression for expression) or
     ``nufft`` (the fast approximate form of the matched filter and the signal

@@ -55,8 +55,9 @@ extern "C" {
  *        reference's summation order per output element.  Judged against the
  *        reference kernels (relative L2 <= 1e-5).
  * MIXED: carrier phase f0*tau reduced modulo one cycle in FP64, per-sample
- *        phasors by an FP32 Horner / rotator recurrence (2 phasors per
- *        (voxel|point, antenna) instead of one per sample), compensated
+ *        sums by FP32 recurrences (second-order Goertzel, three-term
+ *        Chebyshev, packed Horner; a few phasors per (voxel|point, antenna)
+ *        instead of one per sample), compensated
  *        (Kahan) accumulation across antennas.  Judged against an FP64 oracle
  *        (relative L2 <= 1e-4).                                              */
 #define GERAF_MODE_PLAIN 0
